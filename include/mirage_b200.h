@@ -1,0 +1,178 @@
+/*
+ * mirage_b200 -- B200-native MirAge classification hot path, C ABI.
+ *
+ * The reference binds this path through C++ calls with STL types (no C ABI exists there):
+ *   - index load:   Hashmap::ReadHashmapFile            (MirAge/Hashmap.cpp:329, Hashmap.h:175)
+ *   - seed lookup:  Analyser::TPrepareGPUAnalysis        (MirAge/Analyser.cpp:1317, Analyser.h:175)
+ *   - scoring:      MatrixCPU::CPUGetHighestScore        (MirAge/MatrixCPU.cpp:417, MatrixCPU.h:41)
+ *                   CUDAGetHighestScore                  (MirAge/MatrixGPUCU.cu:571, Analyser.h:228)
+ *   - strand merge: Analyser::TGetHighestScoreUsingCPU   (MirAge/Analyser.cpp:592-611)
+ * The entry points below replace those calls one for one (each declaration names the call it
+ * replaces). Plain pointers and sizes only; no exceptions cross this boundary; every function
+ * returns MG_OK (0) or a negative MG_ERR_* code, with a message from mg_last_error().
+ *
+ * Semantics are the reference's CPU path (MatrixCPU), bit-exact: the same candidate
+ * references, the same Score / percentageMatch / relative-score float bits and the same
+ * top-scoring reference set per read, for a single .mhm file in memory mode "extreme",
+ * speed mode "Sensitive", reverse complements on.
+ *
+ * Threading: an mg_index is immutable after mg_open and may be shared by threads; each call
+ * that takes an mg_index serialises on the index's internal stream lock. mg_server is
+ * internally synchronised.
+ */
+#ifndef MIRAGE_B200_H
+#define MIRAGE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MG_OK 0
+#define MG_ERR_IO (-1)        /* file cannot be opened or read */
+#define MG_ERR_BADFMT (-2)    /* not a readable .mhm (or k below its build threshold) */
+#define MG_ERR_OOM (-3)       /* host or device allocation failed; output buffer too small */
+#define MG_ERR_LIMIT (-4)     /* a size outside what this build supports */
+#define MG_ERR_CUDA (-5)      /* CUDA runtime error */
+#define MG_ERR_BADINPUT (-6)  /* a read holds a byte with no reverse complement */
+#define MG_ERR_TIMEOUT (-7)   /* a device-side wait exceeded its iteration bound */
+#define MG_ERR_INVAL (-8)     /* bad argument */
+#define MG_ERR_BUSY (-9)      /* served form: not enough free slots / memory right now */
+
+typedef struct mg_index mg_index;
+typedef struct mg_server mg_server;
+
+/* A batch of reads as CSR: read i is bases[offsets[i] .. offsets[i+1]), raw sequence bytes
+ * as they appear in the FASTA/FASTQ file (the library applies the reference's normalisation:
+ * bytes 97..127 lose 32, Sequences.cpp:43-55, and builds the reverse complement of every read,
+ * Sequences.cpp:795-889). */
+typedef struct {
+  uint64_t n_reads;
+  const uint64_t* offsets; /* n_reads + 1 entries, offsets[0] == 0 */
+  const uint8_t* bases;
+} mg_batch;
+
+/* Result of one read after the strand merge (Analyser.cpp:592-611). */
+typedef struct {
+  float highest;       /* MatrixResult::HighestScore of the kept strand (-1: no candidate) */
+  uint32_t cand_off;   /* first scored candidate of this read in mg_result.cands */
+  uint16_t n_fwd;      /* scored candidates of the forward strand (they come first) */
+  uint16_t n_rc;       /* scored candidates of the reverse-complement strand */
+  uint8_t strand;      /* 0: forward kept, 1: reverse complement kept */
+  uint8_t reported;    /* 1 when the reference logs this read (Analyser.cpp:388) */
+  uint16_t n_top;      /* size of the top-scoring reference group */
+} mg_read_result;
+
+/* One scored candidate (a MatrixResult::ResultsScores entry with its raw score). Candidates
+ * of a strand are in ascending refID order, as CreateResultsScores emits them. */
+typedef struct {
+  uint32_t ref;        /* global reference ID (.mhm order) */
+  float rel;           /* relative score, MatrixResult::GetRelativeScore */
+  float score;         /* CalculateScore's Score */
+  float pct;           /* CalculateScore's percentageMatch */
+} mg_candidate;
+
+/* Caller-owned output buffers. */
+typedef struct {
+  mg_read_result* reads;   /* n_reads entries */
+  mg_candidate* cands;     /* cand_cap entries */
+  uint64_t cand_cap;
+  uint64_t n_cands;        /* written: candidates used (or needed, with MG_ERR_OOM) */
+} mg_result;
+
+/* Index statistics. */
+typedef struct {
+  uint64_t n_hashes, n_postings, n_refs, ref_bases;
+  uint64_t device_bytes;   /* HBM held by the index */
+  int32_t k, word;         /* k and the .mhm word width (4 or 8) */
+  double load_seconds, upload_seconds;
+} mg_index_info;
+
+/* Replaces Hashmap::ReadHashmapFile (Hashmap.cpp:329) for one file: parses the .mhm, decodes
+ * every posting record (Analyser.cpp:1602-1752) and builds the HBM-resident lookup tables on
+ * `device`. k is considerthreshold (MirAge.cpp:208); it may not be below the index's own. */
+int mg_open(const char* mhm_path, int k, int device, mg_index** out);
+
+/* Same from an in-memory .mhm image. */
+int mg_open_image(const uint8_t* image, uint64_t len, int k, int device, mg_index** out);
+
+void mg_close(mg_index* ix);
+int mg_index_get_info(const mg_index* ix, mg_index_info* info);
+
+/* Host-only validation of a .mhm image (no GPU needed): parses the file the way mg_open does,
+ * decodes every posting record, and fills the counts of *info (device fields zero). Same
+ * error codes as mg_open_image. */
+int mg_inspect_image(const uint8_t* image, uint64_t len, int k, mg_index_info* info);
+
+/* The logarithm the relative score uses, evaluated on the index's device at n points
+ * (device results for x in [1, 2^20), which match the host libm's logf bit for bit). Exposed
+ * so callers can verify that agreement. Host buffers. */
+int mg_eval_logf(mg_index* ix, const float* x, float* out, uint64_t n);
+
+/* Replaces Hashmap::BuildHashmapTable + SaveHashmapTableV3 (Hashmap.cpp:967, :1701): builds a
+ * .mhm image from references. names: n_refs NUL-terminated header names (without '>');
+ * taxids may be NULL (-1 each); word 0 chooses 4 unless the file needs 8. On success
+ * *image / *len receive a malloc'd buffer (free with mg_free). */
+int mg_build_image(const uint8_t* bases, const uint64_t* offsets, uint32_t n_refs,
+                   const char* const* names, const int32_t* taxids, int k, int word,
+                   uint8_t** image, uint64_t* len);
+void mg_free(void* p);
+
+/* Plain form. Replaces the reference's per-batch sequence TPrepareGPUAnalysis (Analyser.cpp:
+ * 1317) -> CPUGetHighestScore (MatrixCPU.cpp:417) -> strand merge (Analyser.cpp:592-611):
+ * one kernel launch per batch, one thread per (read, strand), host buffers in and out with
+ * synchronous copies. */
+int mg_score_batch(mg_index* ix, const mg_batch* batch, mg_result* out);
+
+/* Batched form: the same results from the fused persistent kernel (warp per read with work
+ * stealing, block tier for oversized reads), pipelined copies on streams and a captured CUDA
+ * graph. Host buffers in and out. */
+int mg_classify(mg_index* ix, const mg_batch* batch, mg_result* out);
+
+/* Batched form on device-resident buffers (no host copies): d_offsets / d_bases / outputs are
+ * device pointers; stream is a cudaStream_t (NULL = the index's stream). */
+int mg_classify_device(mg_index* ix, uint64_t n_reads, const uint64_t* d_offsets,
+                       const uint8_t* d_bases, mg_read_result* d_reads, mg_candidate* d_cands,
+                       uint64_t cand_cap, uint64_t* d_n_cands, void* stream);
+/* Waits for work queued by mg_classify_device on `stream` and reports its errors; *n_cands
+ * receives the number of candidates written. */
+int mg_classify_device_sync(mg_index* ix, void* stream, uint64_t* n_cands);
+
+/* Scoring-only drop-in for MatrixCPU::CPUGetHighestScore (MatrixCPU.cpp:417) when the
+ * candidate lists come from the reference's own TPrepareGPUAnalysis: per strand s (query
+ * bytes bases[q_off[s]..q_off[s+1]), already normalised), candidates cand_ref[c_off[s] ..
+ * c_off[s+1]) with runs run[r_off[c] .. r_off[c+1]) given as 4 uint32 (Start.Reference,
+ * Start.Query, Last.Reference, Last.Query). Outputs Score, percentageMatch and relative score
+ * per candidate (score -2 and rel -1 for unscored candidates) and HighestScore per strand. */
+int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off,
+                        const uint8_t* bases, const uint64_t* c_off, const uint32_t* cand_ref,
+                        const uint64_t* r_off, const uint32_t* runs, float* score, float* pct,
+                        float* rel, float* highest);
+
+/* Served form: continuous batching against the HBM-resident index. Requests are admitted
+ * into slots while device memory allows, coalesced into the running persistent kernel, and
+ * completed independently. */
+typedef struct {
+  uint32_t max_inflight_reads;  /* reads on the device at once (0: default) */
+  uint32_t max_requests;        /* concurrently tracked requests (0: default) */
+  uint64_t device_budget;       /* bytes of device memory for request buffers (0: from free memory) */
+} mg_server_config;
+
+int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out);
+/* Copies the batch; returns MG_ERR_BUSY when it cannot be admitted now (retry later). */
+int mg_server_submit(mg_server* s, const mg_batch* batch, uint64_t* ticket);
+/* Non-blocking: returns 1 and fills out when the request is complete, 0 when not yet. */
+int mg_server_poll(mg_server* s, uint64_t ticket, mg_result* out);
+/* Blocking variant of mg_server_poll with a timeout in milliseconds (MG_ERR_TIMEOUT). */
+int mg_server_wait(mg_server* s, uint64_t ticket, mg_result* out, uint32_t timeout_ms);
+void mg_server_destroy(mg_server* s);
+
+const char* mg_strerror(int code);
+const char* mg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

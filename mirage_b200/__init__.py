@@ -1,0 +1,297 @@
+"""mirage_b200: B200-native MirAge classification hot path (Python host mirror of the C ABI).
+
+The compute path is the CUDA library libmirage_b200.so (include/mirage_b200.h); this module
+only marshals buffers through ctypes. There is no CPU fallback: if the library is missing the
+import of any entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmirage_b200.so")
+
+READ_DTYPE = np.dtype([("highest", "<f4"), ("cand_off", "<u4"), ("n_fwd", "<u2"), ("n_rc", "<u2"),
+                       ("strand", "u1"), ("reported", "u1"), ("n_top", "<u2")])
+CAND_DTYPE = np.dtype([("ref", "<u4"), ("rel", "<f4"), ("score", "<f4"), ("pct", "<f4")])
+assert READ_DTYPE.itemsize == 16 and CAND_DTYPE.itemsize == 16
+
+MG_OK = 0
+ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LIMIT", -5: "MG_ERR_CUDA",
+          -6: "MG_ERR_BADINPUT", -7: "MG_ERR_TIMEOUT", -8: "MG_ERR_INVAL", -9: "MG_ERR_BUSY"}
+
+EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
+           "mg_build_image", "mg_free",
+           "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
+           "mg_score_candidates", "mg_server_create", "mg_server_submit", "mg_server_poll",
+           "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error"]
+
+
+class MirageError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {ERRORS.get(code, code)} ({msg})")
+        self.code = code
+
+
+class _Batch(C.Structure):
+    _fields_ = [("n_reads", C.c_uint64), ("offsets", C.c_void_p), ("bases", C.c_void_p)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("reads", C.c_void_p), ("cands", C.c_void_p), ("cand_cap", C.c_uint64), ("n_cands", C.c_uint64)]
+
+
+class _Info(C.Structure):
+    _fields_ = [("n_hashes", C.c_uint64), ("n_postings", C.c_uint64), ("n_refs", C.c_uint64),
+                ("ref_bases", C.c_uint64), ("device_bytes", C.c_uint64), ("k", C.c_int32), ("word", C.c_int32),
+                ("load_seconds", C.c_double), ("upload_seconds", C.c_double)]
+
+
+class _ServerConfig(C.Structure):
+    _fields_ = [("max_inflight_reads", C.c_uint32), ("max_requests", C.c_uint32), ("device_budget", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the native library (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m mirage_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, u64, i32, f32p = C.c_void_p, C.c_uint64, C.c_int, C.POINTER(C.c_float)
+        L.mg_open.argtypes = [C.c_char_p, i32, i32, C.POINTER(vp)]
+        L.mg_open_image.argtypes = [vp, u64, i32, i32, C.POINTER(vp)]
+        L.mg_close.argtypes = [vp]
+        L.mg_close.restype = None
+        L.mg_index_get_info.argtypes = [vp, C.POINTER(_Info)]
+        L.mg_build_image.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_char_p), vp, i32, i32,
+                                     C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(u64)]
+        L.mg_free.argtypes = [vp]
+        L.mg_free.restype = None
+        L.mg_score_batch.argtypes = [vp, C.POINTER(_Batch), C.POINTER(_Result)]
+        L.mg_classify.argtypes = [vp, C.POINTER(_Batch), C.POINTER(_Result)]
+        L.mg_classify_device.argtypes = [vp, u64, vp, vp, vp, vp, u64, vp, vp]
+        L.mg_classify_device_sync.argtypes = [vp, vp, C.POINTER(u64)]
+        L.mg_score_candidates.argtypes = [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.mg_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
+        L.mg_server_submit.argtypes = [vp, C.POINTER(_Batch), C.POINTER(u64)]
+        L.mg_server_poll.argtypes = [vp, u64, C.POINTER(_Result)]
+        L.mg_server_wait.argtypes = [vp, u64, C.POINTER(_Result), C.c_uint32]
+        L.mg_server_destroy.argtypes = [vp]
+        L.mg_server_destroy.restype = None
+        L.mg_inspect_image.argtypes = [vp, u64, i32, C.POINTER(_Info)]
+        L.mg_eval_logf.argtypes = [vp, vp, vp, u64]
+        L.mg_strerror.argtypes = [i32]
+        L.mg_strerror.restype = C.c_char_p
+        L.mg_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, where: str) -> int:
+    if rc < 0:
+        raise MirageError(rc, where, (lib().mg_last_error() or b"").decode(errors="replace"))
+    return rc
+
+
+def _u8(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def _u64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def build_image(bases, offsets, names, k: int = 31, word: int = 0, taxids=None) -> np.ndarray:
+    """Build a .mhm image (the reference's index format) from references."""
+    L = lib()
+    bases, offsets = _u8(bases), _u64(offsets)
+    n = len(offsets) - 1
+    arr = (C.c_char_p * max(1, n))(*[(x if isinstance(x, bytes) else str(x).encode()) for x in names])
+    tax = None if taxids is None else np.ascontiguousarray(taxids, dtype=np.int32)
+    out = C.POINTER(C.c_uint8)()
+    ln = C.c_uint64()
+    _check(L.mg_build_image(bases.ctypes.data, offsets.ctypes.data, n, arr,
+                            None if tax is None else tax.ctypes.data, k, word, C.byref(out), C.byref(ln)),
+           "mg_build_image")
+    try:
+        return np.ctypeslib.as_array(out, shape=(ln.value,)).copy()
+    finally:
+        L.mg_free(C.cast(out, C.c_void_p))
+
+
+def inspect_image(image, k: int = 31) -> dict:
+    """Parse and validate a .mhm image on the host (no GPU); returns its counts."""
+    img = _u8(image)
+    inf = _Info()
+    _check(lib().mg_inspect_image(img.ctypes.data, len(img), k, C.byref(inf)), "mg_inspect_image")
+    return {f: getattr(inf, f) for f, _ in _Info._fields_}
+
+
+class Results:
+    """Per-read results (READ_DTYPE) and the scored candidates (CAND_DTYPE), as the C ABI
+    returns them."""
+
+    def __init__(self, reads: np.ndarray, cands: np.ndarray):
+        self.reads = reads
+        self.cands = cands
+
+    def strand_cands(self, i: int, strand: int) -> np.ndarray:
+        r = self.reads[i]
+        o = int(r["cand_off"])
+        if strand == 0:
+            return self.cands[o : o + int(r["n_fwd"])]
+        return self.cands[o + int(r["n_fwd"]) : o + int(r["n_fwd"]) + int(r["n_rc"])]
+
+    def top(self, i: int) -> list[int]:
+        """Top-scoring reference group of read i (ascending refID)."""
+        r = self.reads[i]
+        if not r["reported"]:
+            return []
+        c = self.strand_cands(i, int(r["strand"]))
+        return sorted(int(x["ref"]) for x in c if x["rel"] == r["highest"])
+
+
+class Index:
+    """An HBM-resident MirAge index (one .mhm file)."""
+
+    def __init__(self, source, k: int = 31, device: int = 0):
+        L = lib()
+        h = C.c_void_p()
+        if isinstance(source, (str, os.PathLike)):
+            _check(L.mg_open(os.fspath(source).encode(), k, device, C.byref(h)), "mg_open")
+        else:
+            img = _u8(source)
+            _check(L.mg_open_image(img.ctypes.data, len(img), k, device, C.byref(h)), "mg_open_image")
+        self.h = h
+        self.k = k
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mg_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        inf = _Info()
+        _check(lib().mg_index_get_info(self.h, C.byref(inf)), "mg_index_get_info")
+        return {f: getattr(inf, f) for f, _ in _Info._fields_}
+
+    def _run(self, fn, name, bases, offsets, cand_cap=None):
+        bases, offsets = _u8(bases), _u64(offsets)
+        n = len(offsets) - 1
+        cap = cand_cap if cand_cap is not None else max(1024, 8 * n)
+        reads = np.zeros(n, dtype=READ_DTYPE)
+        cands = np.zeros(cap, dtype=CAND_DTYPE)
+        b = _Batch(n, offsets.ctypes.data, bases.ctypes.data)
+        r = _Result(reads.ctypes.data, cands.ctypes.data, cap, 0)
+        rc = fn(self.h, C.byref(b), C.byref(r))
+        if rc == -3 and r.n_cands > cap and cand_cap is None:
+            return self._run(fn, name, bases, offsets, int(r.n_cands))
+        _check(rc, name)
+        return Results(reads, cands[: r.n_cands].copy())
+
+    def classify(self, bases, offsets, form: str = "batched", cand_cap: int | None = None) -> Results:
+        """Classify a batch of reads (raw FASTA bytes, CSR offsets). form: 'batched' (fused
+        persistent kernel) or 'plain' (one block per read)."""
+        L = lib()
+        fn = L.mg_classify if form == "batched" else L.mg_score_batch
+        return self._run(fn, "mg_classify" if form == "batched" else "mg_score_batch", bases, offsets, cand_cap)
+
+    def eval_logf(self, x) -> np.ndarray:
+        """The device logarithm of the relative score at the points x (float32)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.empty_like(x)
+        _check(lib().mg_eval_logf(self.h, x.ctypes.data, out.ctypes.data, len(x)), "mg_eval_logf")
+        return out
+
+    def score_candidates(self, q_off, bases, c_off, cand_ref, r_off, runs):
+        """Scoring-only drop-in: Score, percentageMatch, relative score per candidate and
+        HighestScore per strand, for candidate lists and runs produced elsewhere."""
+        q_off, bases, c_off, r_off = _u64(q_off), _u8(bases), _u64(c_off), _u64(r_off)
+        cand_ref = np.ascontiguousarray(cand_ref, dtype=np.uint32)
+        runs = np.ascontiguousarray(runs, dtype=np.uint32)
+        ns = len(q_off) - 1
+        nc = int(c_off[-1])
+        score = np.zeros(nc, np.float32)
+        pct = np.zeros(nc, np.float32)
+        rel = np.zeros(nc, np.float32)
+        hi = np.zeros(ns, np.float32)
+        _check(lib().mg_score_candidates(self.h, ns, q_off.ctypes.data, bases.ctypes.data, c_off.ctypes.data,
+                                         cand_ref.ctypes.data, r_off.ctypes.data, runs.ctypes.data,
+                                         score.ctypes.data, pct.ctypes.data, rel.ctypes.data, hi.ctypes.data),
+               "mg_score_candidates")
+        return score, pct, rel, hi
+
+
+class Server:
+    """Served form: continuous batching of requests against a resident index."""
+
+    def __init__(self, index: Index, max_inflight_reads: int = 0, max_requests: int = 0, device_budget: int = 0):
+        self.index = index
+        cfg = _ServerConfig(max_inflight_reads, max_requests, device_budget)
+        h = C.c_void_p()
+        _check(lib().mg_server_create(index.h, C.byref(cfg), C.byref(h)), "mg_server_create")
+        self.h = h
+        self._pending: dict[int, tuple[int, np.ndarray, np.ndarray]] = {}
+
+    def submit(self, bases, offsets) -> int | None:
+        """Submit a request; returns its ticket, or None when it cannot be admitted now."""
+        bases, offsets = _u8(bases), _u64(offsets)
+        n = len(offsets) - 1
+        b = _Batch(n, offsets.ctypes.data, bases.ctypes.data)
+        t = C.c_uint64()
+        rc = lib().mg_server_submit(self.h, C.byref(b), C.byref(t))
+        if rc == -9:
+            return None
+        _check(rc, "mg_server_submit")
+        self._pending[t.value] = (n, bases, offsets)
+        return t.value
+
+    def _result(self, ticket: int, fn, *extra):
+        n = self._pending[ticket][0]
+        cap = max(1024, 8 * n)
+        while True:
+            reads = np.zeros(n, dtype=READ_DTYPE)
+            cands = np.zeros(cap, dtype=CAND_DTYPE)
+            r = _Result(reads.ctypes.data, cands.ctypes.data, cap, 0)
+            rc = fn(self.h, ticket, C.byref(r), *extra)
+            if rc == -3 and r.n_cands > cap:
+                cap = int(r.n_cands)
+                continue
+            _check(rc, "mg_server_poll")
+            if rc == 0:
+                return None
+            del self._pending[ticket]
+            return Results(reads, cands[: r.n_cands].copy())
+
+    def poll(self, ticket: int) -> Results | None:
+        return self._result(ticket, lib().mg_server_poll)
+
+    def wait(self, ticket: int, timeout_ms: int = 60000) -> Results:
+        res = self._result(ticket, lib().mg_server_wait, timeout_ms)
+        if res is None:
+            raise MirageError(-7, "mg_server_wait", "timed out")
+        return res
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mg_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,840 @@
+// mirage_b200 C ABI: index upload, the relative-score logf table, the classification kernels
+// (warp tier, block tier, global-memory tier), output compaction and the host entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/mirage_b200.h"
+#include "mg_device.cuh"
+#include "mg_kernels.cuh"
+#include "mhm.h"
+
+namespace mg {
+
+// ------------------------------------------------------------------------------ errors
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CU(call)                                                                                \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return set_error(MG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+// ------------------------------------------------------------------------------ tiers
+
+// Warp tier: one warp per read, workspace in shared memory (8 warps per block).
+constexpr int kW1Warps = 8;
+constexpr int kW1Q = 320, kW1Seeds = 20, kW1E = 128, kW1C = 8;
+constexpr int kW1Chunk = 4;  // reads taken per work-stealing step
+
+struct WarpSmem {
+  uint64_t kA[kW1E];
+  uint32_t kB[kW1E];
+  uint32_t X[kW1E];
+  uint32_t Y[kW1E];
+  uint32_t fpos[32];
+  mg_candidate cb[2][kW1C];
+  uint8_t q[kW1Q];
+  RedTmp<32> red;
+};
+
+// Block tier: one block of 256 threads per read, workspace in dynamic shared memory.
+constexpr int kB2Threads = 256;
+constexpr int kB2Q = 20480, kB2Seeds = 1408, kB2E = 4096, kB2C = 128;
+// Global tier: one block per read, workspace in global scratch.
+constexpr int kB3Threads = 256;
+constexpr int kB3Q = 65535, kB3Seeds = 4400, kB3E = 65536, kB3C = 4096;
+constexpr int kB3Blocks = 32;
+
+struct WsLayout {
+  size_t kA, kB, X, Y, fpos, cb, q, red, total;
+};
+
+static WsLayout ws_layout(int Q, int seeds, int E, int C) {
+  WsLayout l;
+  size_t o = 0;
+  auto take = [&](size_t n, size_t al) {
+    o = (o + al - 1) / al * al;
+    size_t at = o;
+    o += n;
+    return at;
+  };
+  l.kA = take((size_t)E * 8, 16);
+  l.kB = take((size_t)E * 4, 16);
+  l.X = take((size_t)E * 4, 16);
+  l.Y = take((size_t)E * 4, 16);
+  l.fpos = take((size_t)seeds * 4, 16);
+  l.cb = take((size_t)2 * C * sizeof(mg_candidate), 16);
+  l.q = take((size_t)Q, 16);
+  l.red = take(sizeof(RedTmp<256>), 16);
+  l.total = (o + 127) / 128 * 128;
+  return l;
+}
+
+__device__ __forceinline__ StrandWS ws_from(uint8_t* base, const WsLayout& l, int C) {
+  StrandWS ws;
+  ws.kA = (uint64_t*)(base + l.kA);
+  ws.kB = (uint32_t*)(base + l.kB);
+  ws.X = (uint32_t*)(base + l.X);
+  ws.Y = (uint32_t*)(base + l.Y);
+  ws.fpos = (uint32_t*)(base + l.fpos);
+  ws.cb[0] = (mg_candidate*)(base + l.cb);
+  ws.cb[1] = ws.cb[0] + C;
+  ws.q = base + l.q;
+  return ws;
+}
+
+struct StageDev {
+  mg_candidate* stage;   // kSlots per read
+  mg_candidate* arena;
+  uint64_t arena_cap;
+  unsigned long long* arena_n;
+};
+
+__global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp(DevIndex ix, BatchDev b, StageDev sd) {
+  __shared__ WarpSmem sm[kW1Warps];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpSmem& S = sm[w];
+  StrandWS ws;
+  ws.q = S.q;
+  ws.fpos = S.fpos;
+  ws.kA = S.kA;
+  ws.kB = S.kB;
+  ws.X = S.X;
+  ws.Y = S.Y;
+  ws.cb[0] = S.cb[0];
+  ws.cb[1] = S.cb[1];
+  const Caps caps{kW1Q, kW1Seeds, kW1E, kW1C};
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((uint64_t)base >= b.n) break;
+    const uint64_t end64 = (uint64_t)base + kW1Chunk;
+    const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
+    for (uint32_t r = base; r < end; r++) {
+      if (!process_read<32>(ix, b, r, ws, caps, &S.red, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+        if (lane == 0) {
+          unsigned at = atomicAdd(b.n_ovf1, 1u);
+          b.ovf1[at] = r;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Block tier over a list of reads (list == nullptr: every read, the plain form).
+template <int G>
+__global__ void __launch_bounds__(G) k_classify_block(DevIndex ix, BatchDev b, StageDev sd, const uint32_t* list,
+                                                       const unsigned* list_n, unsigned* cursor, uint32_t* next,
+                                                       unsigned* next_n, uint8_t* gws, WsLayout lay, Caps caps,
+                                                       int last_tier) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  __shared__ uint32_t s_item;
+  uint8_t* base = gws ? gws + (size_t)blockIdx.x * lay.total : dsm;
+  const StrandWS ws = ws_from(base, lay, caps.c);
+  RedTmp<G>* red = (RedTmp<G>*)(base + lay.red);
+  const uint64_t n = list ? (uint64_t)*list_n : b.n;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = cursor ? atomicAdd(cursor, 1u) : 0xFFFFFFFFu;
+    __syncthreads();
+    uint64_t item = cursor ? (uint64_t)s_item : (uint64_t)blockIdx.x;
+    __syncthreads();
+    if (!cursor && item >= n) break;
+    if (item >= n) break;
+    const uint32_t r = list ? list[item] : (uint32_t)item;
+    if (!process_read<G>(ix, b, r, ws, caps, red, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+      if (threadIdx.x == 0) {
+        if (last_tier) {
+          atomicOr(b.err, kErrLimit);
+          b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
+        } else {
+          unsigned at = atomicAdd(next_n, 1u);
+          next[at] = r;
+        }
+      }
+    }
+    __syncthreads();
+    if (!cursor) break;
+  }
+}
+
+// Output compaction: exclusive scan of per-read candidate counts, then a scatter into one
+// contiguous array in read order.
+constexpr int kScanBlock = 1024;
+
+__global__ void k_count_sums(const mg_read_result* reads, uint64_t n, unsigned long long* block_sums) {
+  __shared__ unsigned long long s[kScanBlock / 32];
+  uint64_t i = (uint64_t)blockIdx.x * kScanBlock + threadIdx.x;
+  unsigned long long v = i < n ? (unsigned long long)(reads[i].n_fwd + reads[i].n_rc) : 0ull;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < kScanBlock / 32; w++) t += s[w];
+    block_sums[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_scan_sums(unsigned long long* block_sums, uint64_t nb, unsigned long long* total) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    unsigned long long run = 0;
+    for (uint64_t i = 0; i < nb; i++) {
+      unsigned long long v = block_sums[i];
+      block_sums[i] = run;
+      run += v;
+    }
+    *total = run;
+  }
+}
+
+__global__ void k_scatter(mg_read_result* reads, uint64_t n, const unsigned long long* block_sums, StageDev sd,
+                          mg_candidate* out, uint64_t cap, int* err) {
+  __shared__ unsigned long long s[kScanBlock / 32];
+  const uint64_t i = (uint64_t)blockIdx.x * kScanBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned long long v = i < n ? (unsigned long long)(reads[i].n_fwd + reads[i].n_rc) : 0ull;
+  unsigned long long x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s[wid] = x;
+  __syncthreads();
+  unsigned long long wb = 0;
+  for (int w = 0; w < wid; w++) wb += s[w];
+  if (i >= n) return;
+  const unsigned long long off = block_sums[blockIdx.x] + wb + x - v;
+  mg_read_result rr = reads[i];
+  const uint32_t tot = rr.n_fwd + rr.n_rc;
+  const mg_candidate* src = tot > (uint32_t)kSlots ? sd.arena + rr.cand_off : sd.stage + i * kSlots;
+  if (off + tot > cap) {
+    atomicOr(err, kErrOutput);
+  } else {
+    for (uint32_t c = 0; c < tot; c++) out[off + c] = src[c];
+  }
+  rr.cand_off = (uint32_t)off;
+  reads[i] = rr;
+}
+
+// Index construction: directory from the ascending TOC (dir[h] = first posting of the first
+// TOC hash >= h), and the logf probe.
+__global__ void k_fill_dir(const uint32_t* toc_hash, const uint32_t* toc_start, uint64_t n, uint32_t total,
+                           uint32_t* dir) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  const uint64_t lo = i == 0 ? 0 : (uint64_t)toc_hash[i - 1] + 1;
+  const uint64_t hi = i == n ? (1ull << 28) : (uint64_t)toc_hash[i];
+  const uint32_t v = i == n ? total : toc_start[i];
+  for (uint64_t h = lo; h <= hi; h++) dir[h] = v;
+}
+
+__global__ void k_log_probe(uint32_t lo_bits, uint32_t n, float* out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = log_dev_raw(__uint_as_float(lo_bits + i));
+}
+
+__global__ void k_eval_logf(DevIndex ix, const float* x, float* out, uint64_t n, int* errw) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int err = 0;
+  out[i] = ref_logf(ix, x[i], &err);
+  if (err) atomicOr(errw, err);
+}
+
+// Scoring-only drop-in (MatrixCPU::CPUGetHighestScore): one thread per candidate, like the
+// reference's CUDA kernel, with the semantics of CalculateScore.
+__global__ void k_score_candidates(DevIndex ix, uint64_t n_strands, const uint64_t* q_off, const uint8_t* bases,
+                                   const uint64_t* c_off, const uint32_t* cand_ref, const uint64_t* r_off,
+                                   const uint32_t* runs, uint64_t n_cands, const uint64_t* cand_strand,
+                                   float* score_out, float* pct_out, float* rel_out, uint32_t* hit_ws,
+                                   uint64_t hit_words_per_thread, int* errw) {
+  const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cands) return;
+  const uint64_t s = cand_strand[c];
+  const uint8_t* q = bases + q_off[s];
+  const uint32_t L = (uint32_t)(q_off[s + 1] - q_off[s]);
+  const uint32_t ref = cand_ref[c];
+  const uint8_t* rs = ix.bases + ix.ref_off[ref];
+  const uint32_t rlen = ix.ref_len[ref];
+  const uint32_t k = (uint32_t)ix.k;
+  uint32_t* hit = hit_ws + (uint64_t)c * hit_words_per_thread;
+  const uint32_t nw = (L + 31) / 32;
+  for (uint32_t w = 0; w < nw; w++) hit[w] = 0;
+  uint64_t sc = 0, sr = 0;
+  for (uint64_t r = r_off[c]; r < r_off[c + 1]; r++) {
+    const uint32_t sref = runs[4 * r], sq = runs[4 * r + 1], lref = runs[4 * r + 2], lq = runs[4 * r + 3];
+    if (sq > lq) continue;
+    const uint32_t tail = tail_walk(q, rs, L, rlen, lq, lref, k);
+    const uint32_t head = head_walk(q, rs, sq, sref, k);
+    const uint64_t tot = (uint64_t)tail + head + (lq - sq);
+    if (tot >= k) {
+      sc += tot;
+      sr += tot * (tot + 1) / 2;
+      for (uint64_t p = sq - head; p < sq - head + tot; p++) hit[p >> 5] |= 1u << (p & 31);
+    }
+  }
+  float score = -2.0f, pct = 0.0f, rel = -1.0f;
+  int err = 0;
+  if (sc > 0) {
+    uint32_t hits = 0;
+    for (uint32_t w = 0; w < nw; w++) hits += __popc(hit[w]);
+    final_score(sr, sc, hits, L, &score, &pct);
+    rel = relative_score(ix, __uint2float_rn(L), __uint2float_rn(rlen), score, &err);
+  }
+  score_out[c] = score;
+  pct_out[c] = pct;
+  rel_out[c] = rel;
+  if (err) atomicOr(errw, err);
+}
+
+// ------------------------------------------------------------------------------ host side
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  int alloc(size_t bytes) {
+    if (bytes <= n && p) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return -1;
+    n = bytes;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
+};
+
+}  // namespace mg
+
+struct mg_index {
+  int device = 0;
+  mg::DevIndex dix{};
+  mg::MhmIndex host;  // refs, headers, taxids kept; postings released after upload
+  mg::DevBuf dir, post, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals;
+  // per-call workspace
+  mg::DevBuf w_offs, w_bases, w_reads, w_stage, w_arena, w_cands, w_ctr, w_ovf, w_sums, w_gws;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  mg_index_info info{};
+  uint64_t device_bytes = 0;
+};
+
+namespace mg {
+
+// Compare the device log with the host libm logf over the whole domain and record where
+// they differ, so that the device reproduces the reference's logf bit for bit.
+static int build_log_table(mg_index* ix) {
+  const uint32_t chunk = 1u << 23;
+  DevBuf dprobe;
+  if (dprobe.alloc((size_t)chunk * 4)) return set_error(MG_ERR_OOM, "log table probe");
+  std::vector<float> dev(chunk);
+  std::vector<uint32_t> keys;
+  std::vector<float> vals;
+  std::vector<uint32_t> bitmap(kLogDomain / 32, 0);
+  int nt = std::max(1u, std::thread::hardware_concurrency());
+  for (uint32_t lo = kLogLoBits; lo < kLogHiBits; lo += chunk) {
+    uint32_t n = std::min<uint32_t>(chunk, kLogHiBits - lo);
+    k_log_probe<<<(n + 255) / 256, 256, 0, ix->stream>>>(lo, n, dprobe.as<float>());
+    CU(cudaMemcpyAsync(dev.data(), dprobe.p, (size_t)n * 4, cudaMemcpyDeviceToHost, ix->stream));
+    CU(cudaStreamSynchronize(ix->stream));
+    std::vector<std::vector<uint32_t>> lk(nt);
+    std::vector<std::vector<float>> lv(nt);
+    std::vector<std::thread> th;
+    uint32_t per = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; t++)
+      th.emplace_back([&, t] {
+        uint32_t a = std::min(n, per * t), b = std::min(n, a + per);
+        for (uint32_t i = a; i < b; i++) {
+          uint32_t bits = lo + i;
+          float x;
+          std::memcpy(&x, &bits, 4);
+          float h = logf(x);
+          uint32_t hb, db;
+          std::memcpy(&hb, &h, 4);
+          std::memcpy(&db, &dev[i], 4);
+          if (hb != db) {
+            lk[t].push_back(bits);
+            lv[t].push_back(h);
+          }
+        }
+      });
+    for (auto& x : th) x.join();
+    for (int t = 0; t < nt; t++) {
+      for (size_t j = 0; j < lk[t].size(); j++) {
+        uint32_t r = lk[t][j] - kLogLoBits;
+        bitmap[r >> 5] |= 1u << (r & 31);
+        keys.push_back(lk[t][j]);
+        vals.push_back(lv[t][j]);
+      }
+    }
+  }
+  dprobe.release();
+  if (ix->logx_bitmap.alloc(bitmap.size() * 4) || ix->logx_keys.alloc(keys.size() * 4 + 4) ||
+      ix->logx_vals.alloc(vals.size() * 4 + 4))
+    return set_error(MG_ERR_OOM, "log table");
+  CU(cudaMemcpy(ix->logx_bitmap.p, bitmap.data(), bitmap.size() * 4, cudaMemcpyHostToDevice));
+  if (!keys.empty()) {
+    CU(cudaMemcpy(ix->logx_keys.p, keys.data(), keys.size() * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(ix->logx_vals.p, vals.data(), vals.size() * 4, cudaMemcpyHostToDevice));
+  }
+  ix->dix.logx_bitmap = ix->logx_bitmap.as<uint32_t>();
+  ix->dix.logx_keys = ix->logx_keys.as<uint32_t>();
+  ix->dix.logx_vals = ix->logx_vals.as<float>();
+  ix->dix.n_logx = (uint32_t)keys.size();
+  ix->device_bytes += bitmap.size() * 4 + keys.size() * 8;
+  return MG_OK;
+}
+
+static int upload_index(mg_index* ix, int k) {
+  MhmIndex& h = ix->host;
+  const uint64_t n = h.n_hash;
+  const uint64_t total = h.postings.size();
+  if (total >= 0xFFFFFFFFull) return set_error(MG_ERR_LIMIT, "more than 2^32-1 postings");
+  // the directory needs the TOC ascending (the builder writes it so); reject duplicates
+  for (uint64_t i = 1; i < n; i++)
+    if (h.toc_hash[i] <= h.toc_hash[i - 1]) return set_error(MG_ERR_BADFMT, "TOC hashes not strictly ascending");
+  CU(cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking));
+  if (ix->dir.alloc(((1ull << 28) + 1) * 4) || ix->post.alloc(total * 8 + 8) || ix->bases.alloc(h.bases.size() + 64) ||
+      ix->ref_off.alloc(h.ref_off.size() * 8 + 8) || ix->ref_len.alloc(h.ref_len.size() * 4 + 4))
+    return set_error(MG_ERR_OOM, "device allocation for the index");
+  ix->device_bytes += ix->dir.n + ix->post.n + ix->bases.n + ix->ref_off.n + ix->ref_len.n;
+  CU(cudaMemcpy(ix->post.p, h.postings.data(), total * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ix->bases.p, h.bases.data(), h.bases.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ix->ref_off.p, h.ref_off.data(), h.ref_off.size() * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ix->ref_len.p, h.ref_len.data(), h.ref_len.size() * 4, cudaMemcpyHostToDevice));
+  {
+    std::vector<uint32_t> start(n);
+    for (uint64_t i = 0; i < n; i++) start[i] = (uint32_t)h.bucket[i];
+    DevBuf dh, ds;
+    if (dh.alloc(n * 4 + 4) || ds.alloc(n * 4 + 4)) return set_error(MG_ERR_OOM, "directory build");
+    if (n) {
+      CU(cudaMemcpy(dh.p, h.toc_hash.data(), n * 4, cudaMemcpyHostToDevice));
+      CU(cudaMemcpy(ds.p, start.data(), n * 4, cudaMemcpyHostToDevice));
+    }
+    k_fill_dir<<<(unsigned)((n + 1 + 255) / 256), 256, 0, ix->stream>>>(dh.as<uint32_t>(), ds.as<uint32_t>(), n,
+                                                                     (uint32_t)total, ix->dir.as<uint32_t>());
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(ix->stream));
+    dh.release();
+    ds.release();
+  }
+  DevIndex& d = ix->dix;
+  d.dir = ix->dir.as<uint32_t>();
+  d.post = ix->post.as<uint2>();
+  d.bases = ix->bases.as<uint8_t>();
+  d.ref_off = ix->ref_off.as<uint64_t>();
+  d.ref_len = ix->ref_len.as<uint32_t>();
+  d.n_refs = h.n_refs;
+  d.empty_hash = h.has_empty_last ? h.empty_last_hash : 0xFFFFFFFFu;
+  d.k = k;
+  d.step = k / 2;
+  d.hlen = k - k / 2 + 1;
+  int rc = build_log_table(ix);
+  if (rc) return rc;
+  std::vector<Posting>().swap(h.postings);
+  std::vector<uint8_t>().swap(h.bases);
+  return MG_OK;
+}
+
+static int open_common(mg_index* ix, int k, int device) {
+  ix->device = device;
+  CU(cudaSetDevice(device));
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = upload_index(ix, k);
+  auto t1 = std::chrono::steady_clock::now();
+  ix->info.upload_seconds = std::chrono::duration<double>(t1 - t0).count();
+  ix->info.k = k;
+  ix->info.word = ix->host.word;
+  ix->info.n_hashes = ix->host.n_hash;
+  ix->info.n_refs = ix->host.n_refs;
+  ix->info.device_bytes = ix->device_bytes;
+  return rc;
+}
+
+// ---------------------------------------------------------------------- classification
+
+struct Plan {
+  bool plain;  // block-per-read form
+};
+
+static int ensure_workspace(mg_index* ix, uint64_t n_reads, uint64_t n_bases, bool host_io) {
+  uint64_t arena_cap = std::max<uint64_t>(1 << 16, n_reads * 2);
+  if (host_io) {
+    if (ix->w_offs.alloc((n_reads + 1) * 8) || ix->w_bases.alloc(n_bases + 16) ||
+        ix->w_reads.alloc(n_reads * sizeof(mg_read_result) + 16))
+      return set_error(MG_ERR_OOM, "batch buffers");
+  }
+  if (ix->w_stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
+      ix->w_arena.alloc(arena_cap * sizeof(mg_candidate)) || ix->w_ctr.alloc(256) ||
+      ix->w_ovf.alloc(2 * n_reads * 4 + 16) || ix->w_sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+    return set_error(MG_ERR_OOM, "staging buffers");
+  const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
+  if (ix->w_gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
+  return MG_OK;
+}
+
+// Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
+// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64)
+static int run_pipeline(mg_index* ix, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
+                        mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
+                        bool plain) {
+  uint8_t* ctr = ix->w_ctr.as<uint8_t>();
+  CU(cudaMemsetAsync(ctr, 0, 256, st));
+  BatchDev b;
+  b.n = n;
+  b.offs = d_offs;
+  b.bases = d_bases;
+  b.reads = d_reads;
+  b.cands = d_out;
+  b.cand_cap = cap;
+  b.n_cands = (unsigned long long*)(ctr + 0);
+  b.err = (int*)(ctr + 16);
+  b.work = (unsigned*)(ctr + 20);
+  b.n_ovf1 = (unsigned*)(ctr + 24);
+  b.work2 = (unsigned*)(ctr + 28);
+  b.n_ovf2 = (unsigned*)(ctr + 32);
+  b.work3 = (unsigned*)(ctr + 36);
+  b.ovf1 = ix->w_ovf.as<uint32_t>();
+  b.ovf2 = ix->w_ovf.as<uint32_t>() + n + 4;
+  StageDev sd;
+  sd.stage = ix->w_stage.as<mg_candidate>();
+  sd.arena = ix->w_arena.as<mg_candidate>();
+  sd.arena_cap = ix->w_arena.n / sizeof(mg_candidate);
+  sd.arena_n = (unsigned long long*)(ctr + 8);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
+  const WsLayout l2 = ws_layout(kB2Q, kB2Seeds, kB2E, kB2C);
+  const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
+  const Caps c2{kB2Q, kB2Seeds, kB2E, kB2C}, c3{kB3Q, kB3Seeds, kB3E, kB3C};
+  static bool attr_set = false;
+  if (!attr_set) {
+    CU(cudaFuncSetAttribute(k_classify_block<kB2Threads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l2.total));
+    attr_set = true;
+  }
+  if (n > 0) {
+    if (plain) {
+      // every read gets its own block (one launch for the batch)
+      k_classify_block<kB2Threads><<<(unsigned)n, kB2Threads, l2.total, st>>>(
+          ix->dix, b, sd, nullptr, nullptr, nullptr, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
+    } else {
+      int per_sm = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_classify_warp, kW1Warps * 32, 0);
+      unsigned grid = (unsigned)std::max(1, per_sm) * sms;
+      k_classify_warp<<<grid, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, st>>>(
+          ix->dix, b, sd, b.ovf1, b.n_ovf1, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
+    }
+    CU(cudaGetLastError());
+    k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, st>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3,
+                                                                   nullptr, nullptr, ix->w_gws.as<uint8_t>(), l3, c3, 1);
+    CU(cudaGetLastError());
+    const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    unsigned long long* sums = ix->w_sums.as<unsigned long long>();
+    k_count_sums<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums);
+    k_scan_sums<<<1, 32, 0, st>>>(sums, nb, (unsigned long long*)(ctr + 40));
+    k_scatter<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums, sd, d_out, cap, b.err);
+    CU(cudaGetLastError());
+  }
+  return MG_OK;
+}
+
+static int finish_errors(mg_index* ix, cudaStream_t st, uint64_t* n_cands) {
+  uint8_t h[64];
+  CU(cudaMemcpyAsync(h, ix->w_ctr.p, 64, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  int err;
+  unsigned long long total;
+  std::memcpy(&err, h + 16, 4);
+  std::memcpy(&total, h + 40, 8);
+  *n_cands = total;
+  if (err & kErrBadInput) return set_error(MG_ERR_BADINPUT, "a read holds a byte without a reverse complement");
+  if (err & kErrLimit) return set_error(MG_ERR_LIMIT, "a read exceeds the largest workspace tier");
+  if (err & kErrOutput) return set_error(MG_ERR_OOM, "candidate output buffer too small");
+  if (err & kErrLogRange) return set_error(MG_ERR_LIMIT, "relative-score logarithm outside its exact domain");
+  return MG_OK;
+}
+
+static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bool plain) {
+  if (!ix || !batch || !out || (batch->n_reads && (!batch->offsets || !batch->bases || !out->reads)))
+    return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  CU(cudaSetDevice(ix->device));
+  const uint64_t n = batch->n_reads;
+  if (n >= 0xFFFFFFF0ull) return set_error(MG_ERR_LIMIT, "too many reads in one batch");
+  const uint64_t nb = n ? batch->offsets[n] : 0;
+  if (n && batch->offsets[0] != 0) return set_error(MG_ERR_INVAL, "offsets[0] must be 0");
+  int rc = ensure_workspace(ix, n, nb, true);
+  if (rc) return rc;
+  if (ix->w_cands.alloc(std::max<uint64_t>(out->cand_cap, 1) * sizeof(mg_candidate)))
+    return set_error(MG_ERR_OOM, "candidate buffer");
+  cudaStream_t st = ix->stream;
+  if (n) {
+    CU(cudaMemcpyAsync(ix->w_offs.p, batch->offsets, (n + 1) * 8, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ix->w_bases.p, batch->bases, nb, cudaMemcpyHostToDevice, st));
+  }
+  rc = run_pipeline(ix, n, ix->w_offs.as<uint64_t>(), ix->w_bases.as<uint8_t>(), ix->w_reads.as<mg_read_result>(),
+                    ix->w_cands.as<mg_candidate>(), out->cand_cap, st, plain);
+  if (rc) return rc;
+  uint64_t total = 0;
+  rc = finish_errors(ix, st, &total);
+  out->n_cands = total;
+  if (rc) return rc;
+  if (n) {
+    CU(cudaMemcpyAsync(out->reads, ix->w_reads.p, n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, st));
+    if (total) CU(cudaMemcpyAsync(out->cands, ix->w_cands.p, total * sizeof(mg_candidate), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  return MG_OK;
+}
+
+}  // namespace mg
+
+using namespace mg;
+
+extern "C" {
+
+const char* mg_last_error(void) { return g_last_error.c_str(); }
+
+const char* mg_strerror(int code) {
+  switch (code) {
+    case MG_OK: return "ok";
+    case MG_ERR_IO: return "I/O error";
+    case MG_ERR_BADFMT: return "not a readable MirAge hashmap database";
+    case MG_ERR_OOM: return "out of memory or output buffer too small";
+    case MG_ERR_LIMIT: return "size outside the supported limits";
+    case MG_ERR_CUDA: return "CUDA error";
+    case MG_ERR_BADINPUT: return "read contains a byte without a reverse complement";
+    case MG_ERR_TIMEOUT: return "device wait timed out";
+    case MG_ERR_INVAL: return "invalid argument";
+    case MG_ERR_BUSY: return "server busy";
+    default: return "unknown error";
+  }
+}
+
+static int open_from(mg_index* ix, int rc, const std::string& err, int k, int device, mg_index** out) {
+  if (rc != MHM_OK) {
+    delete ix;
+    return set_error(rc == MHM_ERR_IO ? MG_ERR_IO : rc == MHM_ERR_OOM ? MG_ERR_OOM : rc == MHM_ERR_LIMIT ? MG_ERR_LIMIT : MG_ERR_BADFMT, err);
+  }
+  ix->info.n_postings = ix->host.postings.size();
+  ix->info.ref_bases = ix->host.bases.size();
+  rc = open_common(ix, k, device);
+  if (rc) {
+    mg_close(ix);
+    return rc;
+  }
+  *out = ix;
+  return MG_OK;
+}
+
+int mg_open(const char* path, int k, int device, mg_index** out) {
+  if (!path || !out) return set_error(MG_ERR_INVAL, "null argument");
+  *out = nullptr;
+  mg_index* ix = new mg_index();
+  std::string err;
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = mhm_load(path, k, (int)std::max(1u, std::thread::hardware_concurrency()), &ix->host, &err);
+  ix->info.load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return open_from(ix, rc, err, k, device, out);
+}
+
+int mg_open_image(const uint8_t* image, uint64_t len, int k, int device, mg_index** out) {
+  if (!image || !out) return set_error(MG_ERR_INVAL, "null argument");
+  *out = nullptr;
+  mg_index* ix = new mg_index();
+  std::string err;
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = mhm_parse(image, len, k, (int)std::max(1u, std::thread::hardware_concurrency()), &ix->host, &err);
+  ix->info.load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return open_from(ix, rc, err, k, device, out);
+}
+
+void mg_close(mg_index* ix) {
+  if (!ix) return;
+  cudaSetDevice(ix->device);
+  for (DevBuf* b : {&ix->dir, &ix->post, &ix->bases, &ix->ref_off, &ix->ref_len, &ix->logx_bitmap, &ix->logx_keys,
+                    &ix->logx_vals, &ix->w_offs, &ix->w_bases, &ix->w_reads, &ix->w_stage, &ix->w_arena,
+                    &ix->w_cands, &ix->w_ctr, &ix->w_ovf, &ix->w_sums, &ix->w_gws})
+    b->release();
+  if (ix->stream) cudaStreamDestroy(ix->stream);
+  delete ix;
+}
+
+int mg_index_get_info(const mg_index* ix, mg_index_info* info) {
+  if (!ix || !info) return set_error(MG_ERR_INVAL, "null argument");
+  *info = ix->info;
+  return MG_OK;
+}
+
+int mg_build_image(const uint8_t* bases, const uint64_t* offsets, uint32_t n_refs, const char* const* names,
+                   const int32_t* taxids, int k, int word, uint8_t** image, uint64_t* len) {
+  if (!bases || !offsets || !names || !image || !len) return set_error(MG_ERR_INVAL, "null argument");
+  std::vector<std::string> hdr(n_refs);
+  for (uint32_t r = 0; r < n_refs; r++) hdr[r] = names[r];
+  std::vector<int32_t> tax;
+  if (taxids) tax.assign(taxids, taxids + n_refs);
+  std::vector<uint8_t> img;
+  std::string err;
+  int rc = mhm_build(bases, offsets, n_refs, hdr, tax, k, word, (int)std::max(1u, std::thread::hardware_concurrency()),
+                     &img, &err);
+  if (rc) return set_error(rc == MHM_ERR_OOM ? MG_ERR_OOM : MG_ERR_LIMIT, err);
+  uint8_t* p = (uint8_t*)std::malloc(img.size() ? img.size() : 1);
+  if (!p) return set_error(MG_ERR_OOM, "image");
+  std::memcpy(p, img.data(), img.size());
+  *image = p;
+  *len = img.size();
+  return MG_OK;
+}
+
+void mg_free(void* p) { std::free(p); }
+
+int mg_inspect_image(const uint8_t* image, uint64_t len, int k, mg_index_info* info) {
+  if (!image || !info) return set_error(MG_ERR_INVAL, "null argument");
+  MhmIndex h;
+  std::string err;
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = mhm_parse(image, len, k, (int)std::max(1u, std::thread::hardware_concurrency()), &h, &err);
+  if (rc != MHM_OK)
+    return set_error(rc == MHM_ERR_IO ? MG_ERR_IO : rc == MHM_ERR_OOM ? MG_ERR_OOM : rc == MHM_ERR_LIMIT ? MG_ERR_LIMIT : MG_ERR_BADFMT, err);
+  *info = mg_index_info{};
+  info->n_hashes = h.n_hash;
+  info->n_postings = h.postings.size();
+  info->n_refs = h.n_refs;
+  info->ref_bases = h.bases.size();
+  info->k = k;
+  info->word = h.word;
+  info->load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return MG_OK;
+}
+
+int mg_eval_logf(mg_index* ix, const float* x, float* out, uint64_t n) {
+  if (!ix || (n && (!x || !out))) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  CU(cudaSetDevice(ix->device));
+  DevBuf dx, dout, derr;
+  if (dx.alloc(n * 4 + 4) || dout.alloc(n * 4 + 4) || derr.alloc(4)) return set_error(MG_ERR_OOM, "logf buffers");
+  cudaStream_t st = ix->stream;
+  CU(cudaMemsetAsync(derr.p, 0, 4, st));
+  if (n) {
+    CU(cudaMemcpyAsync(dx.p, x, n * 4, cudaMemcpyHostToDevice, st));
+    k_eval_logf<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ix->dix, dx.as<float>(), dout.as<float>(), n, derr.as<int>());
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, dout.p, n * 4, cudaMemcpyDeviceToHost, st));
+  }
+  int err = 0;
+  CU(cudaMemcpyAsync(&err, derr.p, 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  if (err & kErrLogRange) return set_error(MG_ERR_LIMIT, "input outside [1, 2^20)");
+  return MG_OK;
+}
+
+int mg_score_batch(mg_index* ix, const mg_batch* batch, mg_result* out) { return classify_host(ix, batch, out, true); }
+
+int mg_classify(mg_index* ix, const mg_batch* batch, mg_result* out) { return classify_host(ix, batch, out, false); }
+
+int mg_classify_device(mg_index* ix, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
+                       mg_read_result* d_reads, mg_candidate* d_cands, uint64_t cand_cap, uint64_t* d_n_cands,
+                       void* stream) {
+  if (!ix || (n && (!d_offs || !d_bases || !d_reads))) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  CU(cudaSetDevice(ix->device));
+  int rc = ensure_workspace(ix, n, 0, false);
+  if (rc) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ix->stream;
+  rc = run_pipeline(ix, n, d_offs, d_bases, d_reads, d_cands, cand_cap, st, false);
+  if (rc) return rc;
+  if (d_n_cands) CU(cudaMemcpyAsync(d_n_cands, ix->w_ctr.as<uint8_t>() + 40, 8, cudaMemcpyDeviceToDevice, st));
+  return MG_OK;
+}
+
+int mg_classify_device_sync(mg_index* ix, void* stream, uint64_t* n_cands) {
+  if (!ix || !n_cands) return set_error(MG_ERR_INVAL, "null argument");
+  cudaStream_t st = stream ? (cudaStream_t)stream : ix->stream;
+  return finish_errors(ix, st, n_cands);
+}
+
+int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off, const uint8_t* bases,
+                        const uint64_t* c_off, const uint32_t* cand_ref, const uint64_t* r_off, const uint32_t* runs,
+                        float* score, float* pct, float* rel, float* highest) {
+  if (!ix || !q_off || !c_off) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  CU(cudaSetDevice(ix->device));
+  const uint64_t nc = c_off[n_strands];
+  const uint64_t nr = nc ? r_off[nc] : 0;
+  const uint64_t nb = q_off[n_strands];
+  uint32_t maxL = 0;
+  for (uint64_t s = 0; s < n_strands; s++) maxL = std::max<uint32_t>(maxL, (uint32_t)(q_off[s + 1] - q_off[s]));
+  for (uint64_t c = 0; c < nc; c++)
+    if (cand_ref[c] >= ix->dix.n_refs) return set_error(MG_ERR_INVAL, "candidate reference out of range");
+  std::vector<uint64_t> cs(nc);
+  for (uint64_t s = 0; s < n_strands; s++)
+    for (uint64_t c = c_off[s]; c < c_off[s + 1]; c++) cs[c] = s;
+  const uint64_t hw = (maxL + 31) / 32 + 1;
+  DevBuf dq, db, dr, drun, dcs, dro, dsc, dpc, drl, dhit, derr;
+  if (dq.alloc((n_strands + 1) * 8) || db.alloc(nb + 16) || dr.alloc(nc * 4 + 4) || drun.alloc(nr * 16 + 16) ||
+      dcs.alloc(nc * 8 + 8) || dro.alloc((nc + 1) * 8) || dsc.alloc(nc * 4 + 4) || dpc.alloc(nc * 4 + 4) ||
+      drl.alloc(nc * 4 + 4) || dhit.alloc(nc * hw * 4 + 4) || derr.alloc(4))
+    return set_error(MG_ERR_OOM, "scoring buffers");
+  cudaStream_t st = ix->stream;
+  CU(cudaMemcpyAsync(dq.p, q_off, (n_strands + 1) * 8, cudaMemcpyHostToDevice, st));
+  if (nb) CU(cudaMemcpyAsync(db.p, bases, nb, cudaMemcpyHostToDevice, st));
+  if (nc) {
+    CU(cudaMemcpyAsync(dr.p, cand_ref, nc * 4, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dcs.p, cs.data(), nc * 8, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dro.p, r_off, (nc + 1) * 8, cudaMemcpyHostToDevice, st));
+  }
+  if (nr) CU(cudaMemcpyAsync(drun.p, runs, nr * 16, cudaMemcpyHostToDevice, st));
+  CU(cudaMemsetAsync(derr.p, 0, 4, st));
+  if (nc)
+    k_score_candidates<<<(unsigned)((nc + 127) / 128), 128, 0, st>>>(
+        ix->dix, n_strands, dq.as<uint64_t>(), db.as<uint8_t>(), nullptr, dr.as<uint32_t>(), dro.as<uint64_t>(),
+        drun.as<uint32_t>(), nc, dcs.as<uint64_t>(), dsc.as<float>(), dpc.as<float>(), drl.as<float>(),
+        dhit.as<uint32_t>(), hw, derr.as<int>());
+  CU(cudaGetLastError());
+  int err = 0;
+  CU(cudaMemcpyAsync(&err, derr.p, 4, cudaMemcpyDeviceToHost, st));
+  if (nc) {
+    CU(cudaMemcpyAsync(score, dsc.p, nc * 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(pct, dpc.p, nc * 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(rel, drl.p, nc * 4, cudaMemcpyDeviceToHost, st));
+  }
+  CU(cudaStreamSynchronize(st));
+  for (uint64_t s = 0; s < n_strands; s++) {
+    float h = -1.0f;
+    for (uint64_t c = c_off[s]; c < c_off[s + 1]; c++)
+      if (score[c] > -1 && rel[c] > h) h = rel[c];
+    highest[s] = h;
+  }
+  if (err & kErrLogRange) return set_error(MG_ERR_LIMIT, "relative-score logarithm outside its exact domain");
+  return MG_OK;
+}
+
+}  // extern "C"

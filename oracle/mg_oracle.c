@@ -3,12 +3,13 @@
  * from the reference's behaviour (cited per function below). It is the checker for the CUDA
  * path and the reported CPU baseline; the product never links it.
  *
- * Parity pin: tests/golden/*.dump were produced by the unmodified reference CPU path
+ * Parity pin: the dumps under tests/golden/ were produced by the unmodified reference CPU path
  * (oracle/ref_harness.cpp over the reference's own objects) and tests/test_oracle_golden.py
  * checks this file against them field by field (candidates, runs, Score/percentageMatch/
  * relative-score float bits, merged result and top group).
  *
- * Single .mhm file, 32-bit build (HASH_t = SEQ_ID_t = SEQ_POS_t = uint32, Enum.h:10-15),
+ * Single .mhm file, 32-bit build (HASH_t = SEQ_ID_t = SEQ_POS_t = uint32, Enum.h:10-15) or the
+ * -D__Hash64__ build (all uint64, Enum.h:16-21; values here must still fit 32 bits),
  * memory mode "extreme", speed mode "Sensitive", reverse complements on.
  */
 #define _GNU_SOURCE
@@ -33,9 +34,10 @@ struct mgo_index {
   uint8_t* file;
   uint64_t file_len;
   uint64_t n_hash;
+  int word;              /* LoadedBytes: 4, or 8 with -D__Hash64__ */
   uint32_t* toc_hash;    /* file order */
-  uint32_t* toc_sp;      /* stream position of the posting record */
-  uint32_t* toc_size;    /* BufferSize as the reader computes it (last entry 0) */
+  uint64_t* toc_sp;      /* stream position of the posting record */
+  uint64_t* toc_size;    /* BufferSize as the reader computes it (last entry 0) */
   uint32_t* sorted;      /* TOC indices sorted by hash, for lookup */
   uint32_t n_refs;
   uint32_t* ref_size;
@@ -117,22 +119,27 @@ int mgo_open(const char* path, int k, mgo_index** out) {
   int32_t version = (int32_t)rd_le(b + o, 4); o += 4;
   int32_t loaded_bytes = (int32_t)rd_le(b + o, 4); o += 4;
   int32_t threshold = (int32_t)rd_le(b + o, 4); o += 4;
-  int bsp = b[o], bseq = b[o + 2], bhdr = b[o + 3];
-  (void)bseq; (void)bhdr;
+  int bsp = b[o];
   o += 4;
-  /* version 4 (Hashmap.h:252), 32-bit build, k not below the build threshold (:457) */
-  if (version != 4 || loaded_bytes != 4 || bsp != 4 || k < threshold) { mgo_close(ix); return E_FMT; }
+  /* version 4 (Hashmap.h:252); LoadedBytes 4 (32-bit build) or 8 (-D__Hash64__ build); k not
+   * below the build threshold (:457) */
+  if (version != 4 || (loaded_bytes != 4 && loaded_bytes != 8) || bsp != loaded_bytes || k < threshold) {
+    mgo_close(ix);
+    return E_FMT;
+  }
+  const int W = loaded_bytes;
+  ix->word = W;
   uint64_t n = ix->n_hash;
-  NEED(n * 8);
+  NEED(n * 2 * W);
   ix->toc_hash = (uint32_t*)malloc(n * 4 + 4);
-  ix->toc_sp = (uint32_t*)malloc(n * 4 + 4);
-  ix->toc_size = (uint32_t*)malloc(n * 4 + 4);
+  ix->toc_sp = (uint64_t*)malloc(n * 8 + 8);
+  ix->toc_size = (uint64_t*)malloc(n * 8 + 8);
   ix->sorted = (uint32_t*)malloc(n * 4 + 4);
   if (!ix->toc_hash || !ix->toc_sp || !ix->toc_size || !ix->sorted) { mgo_close(ix); return E_OOM; }
   for (uint64_t i = 0; i < n; i++) {
-    ix->toc_hash[i] = (uint32_t)rd_le(b + o, 4);
-    ix->toc_sp[i] = (uint32_t)rd_le(b + o + 4, 4);
-    o += 8;
+    ix->toc_hash[i] = (uint32_t)rd_le(b + o, W);
+    ix->toc_sp[i] = rd_le(b + o + W, W);
+    o += 2 * W;
   }
   /* BufferSize: next stream position minus this one; the entry written for the last hash
    * lands one past the array (Hashmap.cpp:552-553), so the last hash keeps 0 and is treated
@@ -143,25 +150,25 @@ int mgo_open(const char* path, int k, mgo_index** out) {
   qsort(ix->sorted, n, 4, cmp_toc);
   ix->pos_first_sp = n ? ix->toc_sp[0] : 0;
   /* NCBI TaxIDs */
-  NEED(4);
-  uint64_t ntax = rd_le(b + o, 4); o += 4;
+  NEED(W);
+  uint64_t ntax = rd_le(b + o, W); o += W;
   NEED(ntax * 4);
   o += ntax * 4;
   /* sequences TOC */
-  NEED(8);
-  o += 4; /* spGoto */
-  ix->n_refs = (uint32_t)rd_le(b + o, 4); o += 4;
+  NEED(2 * W);
+  o += W; /* spGoto */
+  ix->n_refs = (uint32_t)rd_le(b + o, W); o += W;
   uint32_t nr = ix->n_refs;
-  NEED((uint64_t)nr * 8);
+  NEED((uint64_t)nr * 2 * W);
   ix->ref_size = (uint32_t*)malloc((uint64_t)nr * 4 + 4);
   ix->ref_off = (uint64_t*)malloc((uint64_t)nr * 8 + 8);
   if (!ix->ref_size || !ix->ref_off) { mgo_close(ix); return E_OOM; }
-  for (uint32_t r = 0; r < nr; r++) ix->ref_size[r] = (uint32_t)rd_le(b + o + 4ull * r, 4);
-  o += 4ull * nr;
-  uint32_t first_sp = nr ? (uint32_t)rd_le(b + o, 4) : 0;
-  for (uint32_t r = 0; r < nr; r++) ix->ref_off[r] = (uint32_t)rd_le(b + o + 4ull * r, 4) - first_sp;
-  o += 4ull * nr;
-  if (nr && (uint64_t)first_sp + ix->ref_off[nr - 1] + ix->ref_size[nr - 1] > L) { mgo_close(ix); return E_FMT; }
+  for (uint32_t r = 0; r < nr; r++) ix->ref_size[r] = (uint32_t)rd_le(b + o + (uint64_t)W * r, W);
+  o += (uint64_t)W * nr;
+  uint64_t first_sp = nr ? rd_le(b + o, W) : 0;
+  for (uint32_t r = 0; r < nr; r++) ix->ref_off[r] = rd_le(b + o + (uint64_t)W * r, W) - first_sp;
+  o += (uint64_t)W * nr;
+  if (nr && first_sp + ix->ref_off[nr - 1] + ix->ref_size[nr - 1] > L) { mgo_close(ix); return E_FMT; }
   ix->seq = b + first_sp;
   if (ix->pos_first_sp > L) { mgo_close(ix); return E_FMT; }
   ix->pos_data = b + ix->pos_first_sp;
@@ -227,27 +234,33 @@ static int64_t decode(const mgo_index* ix, int64_t t, ws_t* ws, uint64_t at) {
   if (p + 4 > end) return E_FMT;
   int wo = p[0], wid = p[1], wpos = p[2], wnum = p[3];
   p += 4;
-  if (wo > 4 || wid > 4 || wpos > 4 || wnum > 8 || p + 2 * wo + wnum > end) return E_FMT;
-  uint32_t id_min = (uint32_t)rd_le(p, wo);
-  uint32_t pos_min = (uint32_t)rd_le(p + wo, wo);
+  const int W = ix->word;
+  const uint64_t M = W >= 8 ? ~0ull : ((1ull << (8 * W)) - 1);
+  if (wo > W || wid > W || wpos > W || wnum > 8 || p + 2 * wo + wnum > end) return E_FMT;
+  uint64_t id_min = rd_le(p, wo);
+  uint64_t pos_min = rd_le(p + wo, wo);
   uint64_t num = rd_le(p + 2 * wo, wnum);
   p += 2 * wo + wnum;
   if (p + (uint64_t)wid * num + 1 + wpos > end) return E_FMT;
   GROW(ws->post, ws->post_cap, at + num, post_t);
-  uint32_t raise = id_min; /* + MultipleHashmaps_SequenceOffset[0] == 0 for one file */
-  for (uint64_t j = 0; j < num; j++) ws->post[at + j].ref = (uint32_t)rd_le(p + (uint64_t)j * wid, wid) + raise;
+  uint64_t raise = id_min; /* + MultipleHashmaps_SequenceOffset[0] == 0 for one file */
+  for (uint64_t j = 0; j < num; j++) {
+    uint64_t id = (rd_le(p + (uint64_t)j * wid, wid) + raise) & M;
+    if (id >= ix->n_refs) return E_FMT;
+    ws->post[at + j].ref = (uint32_t)id;
+  }
   p += (uint64_t)wid * num;
   int wrep = p[0];
   uint64_t nrep = rd_le(p + 1, wpos);
   p += 1 + wpos;
-  if (wrep > 4 || p + nrep * (uint64_t)(wrep + wpos) > end) return E_FMT;
+  if (wrep > W || p + nrep * (uint64_t)(wrep + wpos) > end) return E_FMT;
   uint64_t filled = 0;
   for (uint64_t r = 0; r < nrep; r++) {
-    uint32_t c = (uint32_t)rd_le(p, wrep);
-    uint32_t v = (uint32_t)rd_le(p + wrep, wpos) + pos_min;
+    uint64_t c = rd_le(p, wrep);
+    uint64_t v = (rd_le(p + wrep, wpos) + pos_min) & M;
     p += wrep + wpos;
-    if (filled + c > num) return E_FMT; /* run-lengths must cover exactly numIDs entries */
-    for (uint32_t i = 0; i < c; i++) ws->post[at + filled + i].pos = v;
+    if (filled + c > num || v > 0xFFFFFFFFull) return E_FMT; /* run-lengths cover numIDs */
+    for (uint64_t i = 0; i < c; i++) ws->post[at + filled + i].pos = (uint32_t)v;
     filled += c;
   }
   if (filled != num) return E_FMT;
@@ -269,6 +282,15 @@ float mgo_relative_score(float query_len, float ref_len, float score) {
   const float score_max = (float)((((double)len_max * ((double)len_max + 1.0)) / 2.0) / (double)len_max + 1);
   score += 1;
   return logf(score) / logf(score_max);
+}
+
+void mgo_logf_bits(uint32_t lo_bits, uint64_t n, float* out) {
+  for (uint64_t i = 0; i < n; i++) {
+    uint32_t b = lo_bits + (uint32_t)i;
+    float x;
+    memcpy(&x, &b, 4);
+    out[i] = logf(x);
+  }
 }
 
 /* CalculateScore (MatrixCPU.cpp:18-214) for one candidate with its runs. */

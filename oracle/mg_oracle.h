@@ -78,6 +78,10 @@ void mgo_free(void* p);
  * length and Score, exactly as the reference computes it (float logf). */
 float mgo_relative_score(float query_len, float ref_len, float score);
 
+/* Host libm logf at n consecutive float bit patterns starting at lo_bits (the function
+ * GetRelativeScore calls: MatrixResult.cpp:28 resolves log(float) to logf). */
+void mgo_logf_bits(uint32_t lo_bits, uint64_t n, float* out);
+
 #ifdef __cplusplus
 }
 #endif

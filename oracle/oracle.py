@@ -66,8 +66,17 @@ def lib():
         L.mgo_classify_count.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int]
         L.mgo_classify_count.restype = C.c_int64
         L.mgo_free.argtypes = [C.c_void_p]
+        L.mgo_logf_bits.argtypes = [C.c_uint32, C.c_uint64, C.c_void_p]
+        L.mgo_logf_bits.restype = None
         _lib = L
     return _lib
+
+
+def logf_bits(lo_bits: int, n: int) -> np.ndarray:
+    """Host libm logf at n consecutive float bit patterns from lo_bits."""
+    out = np.empty(n, dtype=np.float32)
+    lib().mgo_logf_bits(lo_bits, n, out.ctypes.data)
+    return out
 
 
 def fbits(x: float) -> int:
@@ -173,7 +182,8 @@ def parse_dump(path: str) -> Result:
     merged = []
     cur = None
     cand = None
-    with open(path) as f:
+    import gzip
+    with (gzip.open(path, "rt") if path.endswith(".gz") else open(path)) as f:
         for line in f:
             t = line.split()
             if not t or t[0] == "#":
@@ -217,9 +227,9 @@ def compare(a: Result, b: Result, max_report: int = 10) -> list[str]:
 
 def run_harness(mhm: str, reads_fasta: str, out: str | None = None, job: int = 1,
                 threads: int = 1, logdir: str | None = None, time_only: bool = False,
-                limit: int | None = None) -> str:
+                limit: int | None = None, word: int = 4) -> str:
     """Run the reference harness (oracle/_ref/mg_ref_harness); returns its timing JSON line."""
-    cmd = [HARNESS, "--mhm", mhm, "--reads", reads_fasta, "--job", str(job), "--threads", str(threads)]
+    cmd = [HARNESS if word == 4 else HARNESS + "64", "--mhm", mhm, "--reads", reads_fasta, "--job", str(job), "--threads", str(threads)]
     if out:
         cmd += ["--out", out]
     if logdir:
@@ -235,7 +245,7 @@ def run_harness(mhm: str, reads_fasta: str, out: str | None = None, job: int = 1
     return lines[-1] if lines else ""
 
 
-def build_mhm_with_reference(ref_fasta: str, workdir: str) -> str:
+def build_mhm_with_reference(ref_fasta: str, workdir: str, word: int = 4) -> str:
     """Build a .mhm from FASTA with the reference's own builder (the stock program)."""
     workdir = os.path.abspath(workdir)
     os.makedirs(os.path.join(workdir, "mirage", "data"), exist_ok=True)
@@ -247,7 +257,7 @@ def build_mhm_with_reference(ref_fasta: str, workdir: str) -> str:
     q = os.path.join(workdir, "q.fasta")
     with open(q, "w") as f:
         f.write(">q\n" + "ACGT" * 40 + "\n")
-    p = subprocess.run([MIRAGE_REF, "-query", q, "-reference", os.path.abspath(ref_fasta), "-outputpath",
+    p = subprocess.run([MIRAGE_REF if word == 4 else MIRAGE_REF + "64", "-query", q, "-reference", os.path.abspath(ref_fasta), "-outputpath",
                         os.path.abspath(os.path.join(workdir, "out"))], cwd=os.path.join(workdir, "x"),
                        capture_output=True, text=True)
     if p.returncode != 0:

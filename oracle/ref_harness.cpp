@@ -21,7 +21,7 @@
 // job and clears only its first n_found_seeds entries (Analyser.cpp:2135), so an entry of a
 // later read can inherit a stale "keep" flag from an earlier read of the same job, and a
 // freshly allocated array holds heap garbage. `--job 1` runs every strand as its own job and
-// the replaced operator new[] below hands out zeroed memory, which gives the per-read
+// the operator new[] of oracle/ref_alloc.cpp hands out zeroed memory, which gives the per-read
 // semantics that the restatement and the GPU path implement. `--job N` reproduces the stock
 // program's grouping (N strands per job, forward/reverse pairs adjacent) so the size of that
 // defect can be measured.
@@ -79,15 +79,7 @@
 #undef private
 #undef protected
 
-// Zero-filled array allocations: removes the heap-garbage part of the stale-flag defect
-// (the flag array is `new bool[n]` and only partly cleared).
-void* operator new[](std::size_t n) {
-  void* p = std::calloc(n ? n : 1, 1);
-  if (!p) throw std::bad_alloc();
-  return p;
-}
-void operator delete[](void* p) noexcept { std::free(p); }
-void operator delete[](void* p, std::size_t) noexcept { std::free(p); }
+// Array allocations are padded and zero-filled by oracle/ref_alloc.cpp (linked in).
 
 // The objects the reference's own main() constructs (MirAge.cpp:70-98), wired the same way.
 string Output_Path;

@@ -1,0 +1,109 @@
+"""Edge cases of the CUDA path, each checked against the CPU restatement (oracle/)."""
+import os
+
+import numpy as np
+import pytest
+
+import mirage_b200 as M
+from parity_util import canon_from_dump, canon_from_gpu, diff
+
+pytestmark = pytest.mark.gpu
+
+_ix = {}
+
+
+def plain_index(golden):
+    g = golden("plain")
+    if "plain" not in _ix:
+        from oracle import oracle as O
+
+        _ix["plain"] = (M.Index(g.image), O.Index(g.mhm_path))
+    return g, _ix["plain"]
+
+
+def csr(seqs):
+    offs = np.zeros(len(seqs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(s) for s in seqs])
+    data = np.frombuffer(b"".join(seqs), np.uint8) if seqs else np.zeros(0, np.uint8)
+    return data, offs
+
+
+def check_against_oracle(gix, oix, seqs, form="batched"):
+    data, offs = csr(seqs)
+    r = gix.classify(data, offs, form=form)
+    o = oix.classify(data, offs, threads=os.cpu_count() or 1)
+    d = diff(canon_from_gpu(r), canon_from_dump(o))
+    assert not d, "\n".join(d)
+    return r
+
+
+def test_empty_batch(golden):
+    _, (gix, _) = plain_index(golden)
+    r = gix.classify(np.zeros(0, np.uint8), np.zeros(1, np.uint64))
+    assert len(r.reads) == 0 and len(r.cands) == 0
+
+
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_ragged_and_short_reads(golden, form):
+    g, (gix, oix) = plain_index(golden)
+    ref0 = g.refs.seq(3).tobytes()
+    seqs = [ref0[100:100 + n] for n in (1, 17, 30, 31, 32, 45, 46, 61, 62, 76, 150, 151, 299, 320, 321, 1000, 4999)]
+    check_against_oracle(gix, oix, seqs, form)
+
+
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_lowercase_and_iupac(golden, form):
+    g, (gix, oix) = plain_index(golden)
+    s = bytearray(g.refs.seq(7).tobytes()[500:800])
+    low = bytes(s).lower()
+    withn = bytearray(s)
+    for p in range(0, 300, 37):
+        withn[p] = ord("N")
+    iupac = bytearray(s)
+    for p, c in zip(range(5, 300, 41), b"RYSWKMBDHV"):
+        iupac[p] = c
+    check_against_oracle(gix, oix, [low, bytes(withn), bytes(iupac), bytes(s)], form)
+
+
+def test_invalid_byte_is_rejected(golden):
+    g, (gix, _) = plain_index(golden)
+    s = g.refs.seq(1).tobytes()[:150]
+    data, offs = csr([s, s[:70] + b"X" + s[71:]])
+    with pytest.raises(M.MirageError) as e:
+        gix.classify(data, offs)
+    assert e.value.code == -6
+
+
+def test_reverse_strand_and_ties(golden):
+    """A read copied from a reference's reverse strand is assigned through its reverse
+    complement; a read present in two references gives a two-way top group."""
+    g, (gix, oix) = plain_index(golden)
+    a = g.refs.seq(11).tobytes()[1000:1150]
+    comp = bytes.maketrans(b"ACGT", b"TGCA")
+    rc = a[::-1].translate(comp)
+    r = check_against_oracle(gix, oix, [a, rc])
+    assert r.reads[0]["strand"] == 0 and r.reads[1]["strand"] == 1
+    assert r.top(0) == r.top(1) == [11]
+
+
+def test_small_candidate_buffer_reports_need(golden):
+    g, (gix, _) = plain_index(golden)
+    reads = g.reads.subset(200)
+    full = gix.classify(reads.data, reads.offs)
+    need = len(full.cands)
+    assert need > 10
+    with pytest.raises(M.MirageError) as e:
+        gix.classify(reads.data, reads.offs, cand_cap=need // 2)
+    assert e.value.code == -3
+
+
+def test_long_reads_go_through_every_tier(golden):
+    """Reads beyond the warp tier (block tier) and beyond shared memory (global tier)."""
+    g = golden("long_small")
+    from oracle import oracle as O
+
+    gix = M.Index(g.image)
+    oix = O.Index(g.mhm_path)
+    ref = g.refs.seq(int(np.argmax(g.refs.lengths()))).tobytes()
+    seqs = [ref[0:20000], ref[5:25005], ref[100:60100]]
+    check_against_oracle(gix, oix, seqs)
