@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""Benchmark of the MirAge classification hot path on B200.
+
+Workload ("uneven", the BASELINE config that fits one GPU): 5,000 synthetic references with
+log-normal lengths (median 50 kb, sigma 0.8, ~344 Mbp, GC per reference uniform in [0.3, 0.7]),
+1,000,000 reads per GPU of uniform length 75-300 bp with 0.5% substitutions, 0.1% single-base
+indels and 20% unrelated reads; seeded synthetic data (no public read set is named). A step is
+the classification of one batch of 1,000,000 reads (both strands, seed lookup through best
+reference pick). Inputs (index ~4.6 GB, reads ~187 MB) are larger than the 126 MB L2, so no
+flush is needed between steps.
+
+  value       reads/s with the batch already resident in HBM (fused batched form), device-timed
+              with CUDA events on the launching stream, max over ranks.
+  e2e         reads/s through the C ABI (mg_classify) from pinned host buffers: host->device
+              copy of the reads and device->host copy of every result inside the timed region.
+  plain       the same e2e measurement of the plain form (mg_score_batch, one block per read).
+  roofline    the warp-tier kernel (dominant): algorithmic bytes per launch / its CUDA-event time,
+              against the measured HBM copy bandwidth.
+  cpu_baseline the reference's own CPU path (oracle/_ref harness) when built, else the CPU
+              restatement, on a bounded sample with all host threads.
+
+--impl reference times the reference's CPU implementation of the path (see above) on the same
+workload, one bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 2024
+N_READS = 1_000_000
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi samples (SM clock, throttle reasons) while the timed region runs."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = max(mx, float(f[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        except OSError:
+            pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def hash28_windows_2d(seqs: np.ndarray) -> np.ndarray:
+    """CreateHash24 of equal-length windows (rows of a uint8 matrix)."""
+    x = np.full(seqs.shape[0], 2166136261, dtype=np.uint64)
+    for j in range(seqs.shape[1]):
+        x = ((x * 16777619) & 0xFFFFFFFF) ^ seqs[:, j].astype(np.uint64)
+    return (((x >> 28) ^ x) & 0x0FFFFFFF).astype(np.uint32)
+
+
+def algorithmic_bytes(ix, reads, n_cands: int, k: int = 31) -> dict:
+    """Bytes the path must move per batch (each term one access a minimal implementation
+    cannot avoid): the read bytes; per seed of both strands one 32-byte directory sector and the
+    32-byte sectors holding its postings (8 bytes each); per scored candidate two 32-byte
+    reference windows (head and tail of at least one run); 16 bytes of result per read and per
+    candidate."""
+    step, h = k // 2, k - k // 2 + 1
+    lens = reads.lengths().astype(np.int64)
+    data = reads.data
+    comp = np.zeros(256, np.uint8)
+    for a, b in zip(b"ACGTN", b"TGCAN"):
+        comp[a] = b
+    seed_bytes = 0
+    post_bytes = 0
+    n_seeds = 0
+    for L in np.unique(lens):
+        if L <= k:
+            continue
+        idx = np.flatnonzero(lens == L)
+        starts = reads.offs[idx].astype(np.int64)
+        mat = data[starts[:, None] + np.arange(L)[None, :]]
+        for strand in (0, 1):
+            m = mat if strand == 0 else comp[mat[:, ::-1]]
+            ns = (L - k + step - 1) // step
+            for j in range(ns):
+                hs = hash28_windows_2d(m[:, j * step : j * step + h])
+                cnt = ix.bucket_sizes(hs).astype(np.int64)
+                n_seeds += len(hs)
+                post_bytes += int((((cnt * 8) + 31) // 32 * 32).sum())
+    seed_bytes = 32 * n_seeds
+    read_bytes = int(lens.sum())
+    total = read_bytes + seed_bytes + post_bytes + 64 * n_cands + 16 * len(lens) + 16 * n_cands
+    return {"bytes": total, "read": read_bytes, "directory": seed_bytes, "postings": post_bytes,
+            "ref_windows": 64 * n_cands, "results": 16 * (len(lens) + n_cands), "seeds": n_seeds}
+
+
+def make_workload(scale: float, n_reads: int, rank: int):
+    from mirage_b200 import synth
+
+    # one reference set (seed SEED) for every rank, one read set per rank
+    refs, reads, _ = synth.workload("uneven_fast", scale, seed=SEED, n_reads=n_reads, reads_seed=SEED + 1 + rank)
+    return refs, reads
+
+
+def cpu_baseline(img: np.ndarray, reads, word: int, sample: int) -> dict:
+    """The reference CPU path (oracle harness) on a bounded sample, all host threads; the CPU
+    restatement when the reference harness is not built."""
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    sub = reads.subset(min(sample, len(reads)))
+    with tempfile.TemporaryDirectory(prefix="mg_cpu_") as tmp:
+        mhm = os.path.join(tmp, "index.mhm")
+        img.tofile(mhm)
+        harness = O.HARNESS if word == 4 else O.HARNESS + "64"
+        if os.path.exists(harness):
+            fa = os.path.join(tmp, "reads.fasta")
+            sub.write_fasta(fa)
+            js = json.loads(O.run_harness(mhm, fa, job=1, threads=threads, time_only=True, word=word))
+            return {"value": len(sub) / js["hot_s"], "unit": "reads/s", "cores": threads, "kind": "reference",
+                    "sample": f"{len(sub)} reads of the same workload; reference TPrepareGPUAnalysis + "
+                              f"CPUGetHighestScore + strand merge (index load excluded)"}
+        oix = O.Index(mhm)
+        oix.count(sub.data[: int(sub.offs[min(1000, len(sub))])], sub.offs[: min(1000, len(sub)) + 1], threads)
+        t = time.perf_counter()
+        oix.count(sub.data, sub.offs, threads)
+        dt = time.perf_counter() - t
+        return {"value": len(sub) / dt, "unit": "reads/s", "cores": threads, "kind": "port",
+                "sample": f"{len(sub)} reads of the same workload through the CPU restatement"}
+
+
+def run_reference_arm(args, rank: int, world: int) -> None:
+    """--impl reference: the reference's CPU implementation on host cores."""
+    if rank != 0:
+        return
+    import mirage_b200 as M
+    from oracle import oracle as O
+
+    refs, reads = make_workload(args.scale, args.reads, 0)
+    img = M.build_image(refs.data, refs.offs, refs.headers, k=31)
+    word = int(img[74 + 12])  # the .mhm word width byte
+    threads = os.cpu_count() or 1
+    per_step = args.ref_sample
+    harness = O.HARNESS if word == 4 else O.HARNESS + "64"
+    kind = "reference" if os.path.exists(harness) else "port"
+    times = []
+    with tempfile.TemporaryDirectory(prefix="mg_ref_") as tmp:
+        mhm = os.path.join(tmp, "index.mhm")
+        img.tofile(mhm)
+        del img
+        if kind == "reference":
+            fa = os.path.join(tmp, "reads.fasta")
+            reads.subset(per_step).write_fasta(fa)
+            out = subprocess.run([harness, "--mhm", mhm, "--reads", fa, "--job", "1", "--threads", str(threads),
+                                  "--time", "--repeat", str(args.warmup + args.steps)],
+                                 capture_output=True, text=True, check=True).stderr
+            for line in out.splitlines():
+                if line.startswith('{"rep"'):
+                    times.append(json.loads(line)["hot_s"])
+        else:
+            oix = O.Index(mhm)
+            sub = reads.subset(per_step)
+            for _ in range(args.warmup + args.steps):
+                t = time.perf_counter()
+                oix.count(sub.data, sub.offs, threads)
+                times.append(time.perf_counter() - t)
+    timed = times[args.warmup:]
+    ms = 1000 * float(np.mean(timed))
+    value = per_step / (ms / 1000)
+    line = {"impl": "reference", "metric": "reads/s", "value": value, "unit": "reads/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "uneven: 5000 refs ~344 Mbp log-normal, 1M reads 75-300 bp per GPU",
+                       "sample_reads_per_step": per_step},
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": kind,
+                             "sample": f"{per_step} reads of the workload per step"},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mirage", choices=["mirage", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="shrink the reference set (tests)")
+    ap.add_argument("--reads", type=int, default=N_READS, help="reads per GPU per step")
+    ap.add_argument("--cpu-sample", type=int, default=100_000)
+    ap.add_argument("--ref-sample", type=int, default=100_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import mirage_b200 as M
+
+    t0 = time.time()
+    refs, reads = make_workload(args.scale, args.reads, rank)
+    t_gen = time.time() - t0
+    t0 = time.time()
+    img = M.build_image(refs.data, refs.offs, refs.headers, k=31)
+    t_build = time.time() - t0
+    word = int(img[74 + 12])
+    t0 = time.time()
+    ix = M.Index(img, k=31, device=local)
+    t_open = time.time() - t0
+    info = ix.info()
+    log(f"[rank {rank}] gen {t_gen:.1f}s build {t_build:.1f}s open {t_open:.1f}s index {info}")
+    n = len(reads)
+    n_bases = int(reads.offs[-1])
+    cap = 8 * n + 1024
+
+    # pinned host buffers (the e2e inputs and outputs)
+    h_bases = torch.from_numpy(reads.data).pin_memory()
+    h_offs = torch.from_numpy(reads.offs.view(np.int64)).pin_memory()
+    h_reads = torch.empty(n * 16, dtype=torch.uint8).pin_memory()
+    h_cands = torch.empty(cap * 16, dtype=torch.uint8).pin_memory()
+    # device-resident copies (the `value` inputs)
+    d_bases = h_bases.to(f"cuda:{local}")
+    d_offs = h_offs.to(f"cuda:{local}")
+    d_reads = torch.empty(n * 16, dtype=torch.uint8, device=f"cuda:{local}")
+    d_cands = torch.empty(cap * 16, dtype=torch.uint8, device=f"cuda:{local}")
+    d_nc = torch.zeros(1, dtype=torch.int64, device=f"cuda:{local}")
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+
+    def device_step():
+        ix.classify_device(n, d_offs.data_ptr(), d_bases.data_ptr(), d_reads.data_ptr(), d_cands.data_ptr(), cap,
+                           d_nc.data_ptr(), sp)
+
+    def e2e_step(form="batched"):
+        return ix.classify_ptrs(n, h_offs.data_ptr(), h_bases.data_ptr(), h_reads.data_ptr(), h_cands.data_ptr(), cap,
+                                form)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ix.set_timing(True)
+    for _ in range(args.warmup):
+        device_step()
+        ix.device_sync(sp)
+    barrier()
+    kernel_ms = np.zeros(4)
+    step_ms = []
+    with ClockSampler(local) as clk:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        barrier()
+        with torch.cuda.stream(stream):
+            start.record(stream)
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            device_step()
+            e1.record(stream)
+            n_cands = ix.device_sync(sp)
+            kernel_ms += ix.last_kernel_times()
+            step_ms.append(e0.elapsed_time(e1))
+        end.record(stream)
+        barrier()
+        total_ms = start.elapsed_time(end)
+    total_ms = max_over_ranks(total_ms)
+    ms_per_step = total_ms / args.steps
+    value = world * n / (ms_per_step / 1000)
+
+    # end to end through the C ABI with pinned host buffers
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        n_c = e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t) / args.steps
+    e2e = world * n / e2e_s
+    h2d = n_bases + 8 * (n + 1)
+    d2h = 16 * n + 16 * n_c + 64
+
+    # plain form (one block per read), same e2e measurement
+    for _ in range(2):
+        e2e_step("plain")
+    barrier()
+    t = time.perf_counter()
+    plain_steps = max(1, min(args.steps, 3))
+    for _ in range(plain_steps):
+        e2e_step("plain")
+    torch.cuda.synchronize()
+    plain_s = max_over_ranks(time.perf_counter() - t) / plain_steps
+    plain = world * n / plain_s
+
+    line = None
+    if rank == 0:
+        peaks = measured_peaks()
+        hbm = peaks.get("hbm_gbs")
+        ab = algorithmic_bytes(ix, reads, n_cands)
+        warp_ms = kernel_ms[0] / args.steps
+        achieved = ab["bytes"] / (warp_ms / 1000) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm or 6650.0, "unit": "GB/s",
+                "frac": achieved / (hbm or 6650.0), "traffic": None,
+                "kernel": "k_classify_warp", "kernel_ms": warp_ms,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": ab}
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                cpu = cpu_baseline(img, reads, word, args.cpu_sample)
+            except Exception as e:  # reported, not fatal
+                cpu = {"value": None, "error": str(e)[:200]}
+        line = {"metric": "reads/s", "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+                "config": {"workload": f"uneven: {len(refs)} refs {int(refs.offs[-1])} bp log-normal, "
+                                       f"{n} reads 75-300 bp per GPU (0.5% subs, 0.1% indels, 20% unrelated)",
+                           "index_bytes": len(img), "mhm_word": word, "k": 31,
+                           "l2": "inputs larger than L2 (index + reads), no flush",
+                           "parallelism": f"replicas x{world}, reads sharded"},
+                "e2e": {"value": e2e, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": 1000 * e2e_s, "host_buffers": "pinned"},
+                "plain": {"value": plain, "unit": "reads/s", "ms_per_step": 1000 * plain_s,
+                          "what": "mg_score_batch e2e (one block per read, one launch per batch)"},
+                "batched_over_plain_e2e": e2e / plain,
+                "kernel_ms_per_step": {"warp_tier": warp_ms, "block_tier": kernel_ms[1] / args.steps,
+                                       "global_tier": kernel_ms[2] / args.steps,
+                                       "compaction": kernel_ms[3] / args.steps},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": args.steps * 6,
+                "setup_s": {"generate": t_gen, "index_build": t_build, "open": t_open}}
+        print(json.dumps(line), flush=True)
+    ix.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -111,6 +111,15 @@ int mg_inspect_image(const uint8_t* image, uint64_t len, int k, mg_index_info* i
  * so callers can verify that agreement. Host buffers. */
 int mg_eval_logf(mg_index* ix, const float* x, float* out, uint64_t n);
 
+/* Diagnostics (no counterpart in the reference). mg_set_timing(ix, 1) records CUDA events
+ * around every kernel of each following classification call; mg_last_kernel_times writes the
+ * last call's device times in milliseconds: [warp tier (or the plain form's kernel), block
+ * tier, global-memory tier, output compaction]. mg_bucket_sizes returns the number of
+ * postings stored under each of n 28-bit hashes (the index directory, read on the device). */
+int mg_set_timing(mg_index* ix, int on);
+int mg_last_kernel_times(mg_index* ix, float* ms4);
+int mg_bucket_sizes(mg_index* ix, const uint32_t* hashes, uint32_t* counts, uint64_t n);
+
 /* Replaces Hashmap::BuildHashmapTable + SaveHashmapTableV3 (Hashmap.cpp:967, :1701): builds a
  * .mhm image from references. names: n_refs NUL-terminated header names (without '>');
  * taxids may be NULL (-1 each); word 0 chooses 4 unless the file needs 8. On success

@@ -24,6 +24,7 @@ ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LI
           -6: "MG_ERR_BADINPUT", -7: "MG_ERR_TIMEOUT", -8: "MG_ERR_INVAL", -9: "MG_ERR_BUSY"}
 
 EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
+           "mg_set_timing", "mg_last_kernel_times", "mg_bucket_sizes",
            "mg_build_image", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_server_create", "mg_server_submit", "mg_server_poll",
@@ -85,6 +86,9 @@ def lib() -> C.CDLL:
         L.mg_server_wait.argtypes = [vp, u64, C.POINTER(_Result), C.c_uint32]
         L.mg_server_destroy.argtypes = [vp]
         L.mg_server_destroy.restype = None
+        L.mg_set_timing.argtypes = [vp, i32]
+        L.mg_last_kernel_times.argtypes = [vp, vp]
+        L.mg_bucket_sizes.argtypes = [vp, vp, vp, u64]
         L.mg_inspect_image.argtypes = [vp, u64, i32, C.POINTER(_Info)]
         L.mg_eval_logf.argtypes = [vp, vp, vp, u64]
         L.mg_strerror.argtypes = [i32]
@@ -208,6 +212,44 @@ class Index:
         L = lib()
         fn = L.mg_classify if form == "batched" else L.mg_score_batch
         return self._run(fn, "mg_classify" if form == "batched" else "mg_score_batch", bases, offsets, cand_cap)
+
+    def set_timing(self, on: bool = True) -> None:
+        _check(lib().mg_set_timing(self.h, 1 if on else 0), "mg_set_timing")
+
+    def last_kernel_times(self) -> np.ndarray:
+        """Device ms of the last call: [warp tier or plain kernel, block tier, global tier,
+        output compaction]."""
+        ms = np.zeros(4, np.float32)
+        _check(lib().mg_last_kernel_times(self.h, ms.ctypes.data), "mg_last_kernel_times")
+        return ms
+
+    def bucket_sizes(self, hashes) -> np.ndarray:
+        h = np.ascontiguousarray(hashes, dtype=np.uint32)
+        out = np.empty_like(h)
+        _check(lib().mg_bucket_sizes(self.h, h.ctypes.data, out.ctypes.data, len(h)), "mg_bucket_sizes")
+        return out
+
+    def classify_ptrs(self, n: int, offs_ptr: int, bases_ptr: int, reads_ptr: int, cands_ptr: int,
+                      cand_cap: int, form: str = "batched") -> int:
+        """Classify with caller-provided host pointers (e.g. pinned buffers); returns the number
+        of candidates written."""
+        L = lib()
+        fn = L.mg_classify if form == "batched" else L.mg_score_batch
+        b = _Batch(n, offs_ptr, bases_ptr)
+        r = _Result(reads_ptr, cands_ptr, cand_cap, 0)
+        _check(fn(self.h, C.byref(b), C.byref(r)), "mg_classify")
+        return int(r.n_cands)
+
+    def classify_device(self, n: int, d_offs: int, d_bases: int, d_reads: int, d_cands: int, cand_cap: int,
+                        d_n_cands: int, stream: int = 0) -> None:
+        """Queue the batched form on device buffers (no host copies) on `stream`."""
+        _check(lib().mg_classify_device(self.h, n, d_offs, d_bases, d_reads, d_cands, cand_cap, d_n_cands,
+                                        stream or None), "mg_classify_device")
+
+    def device_sync(self, stream: int = 0) -> int:
+        n = C.c_uint64()
+        _check(lib().mg_classify_device_sync(self.h, stream or None, C.byref(n)), "mg_classify_device_sync")
+        return int(n.value)
 
     def eval_logf(self, x) -> np.ndarray:
         """The device logarithm of the relative score at the points x (float32)."""

@@ -345,6 +345,10 @@ struct mg_index {
   std::mutex mu;
   mg_index_info info{};
   uint64_t device_bytes = 0;
+  // optional per-kernel timing of the last pipeline (events on the launching stream)
+  bool timing = false;
+  bool events_made = false;
+  cudaEvent_t ev[5];
 };
 
 namespace mg {
@@ -539,28 +543,36 @@ static int run_pipeline(mg_index* ix, uint64_t n, const uint64_t* d_offs, const 
     CU(cudaFuncSetAttribute(k_classify_block<kB2Threads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l2.total));
     attr_set = true;
   }
+  const bool tm = ix->timing && ix->events_made;
   if (n > 0) {
+    if (tm) CU(cudaEventRecord(ix->ev[0], st));
     if (plain) {
       // every read gets its own block (one launch for the batch)
       k_classify_block<kB2Threads><<<(unsigned)n, kB2Threads, l2.total, st>>>(
           ix->dix, b, sd, nullptr, nullptr, nullptr, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
+      if (tm) CU(cudaEventRecord(ix->ev[1], st));
+      if (tm) CU(cudaEventRecord(ix->ev[2], st));
     } else {
       int per_sm = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_classify_warp, kW1Warps * 32, 0);
       unsigned grid = (unsigned)std::max(1, per_sm) * sms;
       k_classify_warp<<<grid, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      if (tm) CU(cudaEventRecord(ix->ev[1], st));
       k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, st>>>(
           ix->dix, b, sd, b.ovf1, b.n_ovf1, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
+      if (tm) CU(cudaEventRecord(ix->ev[2], st));
     }
     CU(cudaGetLastError());
     k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, st>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3,
                                                                    nullptr, nullptr, ix->w_gws.as<uint8_t>(), l3, c3, 1);
+    if (tm) CU(cudaEventRecord(ix->ev[3], st));
     CU(cudaGetLastError());
     const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
     unsigned long long* sums = ix->w_sums.as<unsigned long long>();
     k_count_sums<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums);
     k_scan_sums<<<1, 32, 0, st>>>(sums, nb, (unsigned long long*)(ctr + 40));
     k_scatter<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums, sd, d_out, cap, b.err);
+    if (tm) CU(cudaEventRecord(ix->ev[4], st));
     CU(cudaGetLastError());
   }
   return MG_OK;
@@ -685,6 +697,8 @@ void mg_close(mg_index* ix) {
                     &ix->w_cands, &ix->w_ctr, &ix->w_ovf, &ix->w_sums, &ix->w_gws})
     b->release();
   if (ix->stream) cudaStreamDestroy(ix->stream);
+  if (ix->events_made)
+    for (auto& e : ix->ev) cudaEventDestroy(e);
   delete ix;
 }
 
@@ -732,6 +746,53 @@ int mg_inspect_image(const uint8_t* image, uint64_t len, int k, mg_index_info* i
   info->k = k;
   info->word = h.word;
   info->load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return MG_OK;
+}
+
+int mg_set_timing(mg_index* ix, int on) {
+  if (!ix) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  CU(cudaSetDevice(ix->device));
+  if (on && !ix->events_made) {
+    for (auto& e : ix->ev) CU(cudaEventCreate(&e));
+    ix->events_made = true;
+  }
+  ix->timing = on != 0;
+  return MG_OK;
+}
+
+int mg_last_kernel_times(mg_index* ix, float* ms) {
+  if (!ix || !ms) return set_error(MG_ERR_INVAL, "null argument");
+  if (!ix->timing || !ix->events_made) return set_error(MG_ERR_INVAL, "timing is off");
+  for (int i = 0; i < 4; i++) {
+    CU(cudaEventSynchronize(ix->ev[i + 1]));
+    CU(cudaEventElapsedTime(&ms[i], ix->ev[i], ix->ev[i + 1]));
+  }
+  return MG_OK;
+}
+
+__global__ void k_bucket_sizes(const uint32_t* dir, const uint32_t* h, uint32_t* out, uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const uint32_t x = h[i] & 0x0FFFFFFFu;
+    out[i] = dir[x + 1] - dir[x];
+  }
+}
+
+int mg_bucket_sizes(mg_index* ix, const uint32_t* hashes, uint32_t* counts, uint64_t n) {
+  if (!ix || (n && (!hashes || !counts))) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  CU(cudaSetDevice(ix->device));
+  DevBuf dh, dc;
+  if (dh.alloc(n * 4 + 4) || dc.alloc(n * 4 + 4)) return set_error(MG_ERR_OOM, "bucket size buffers");
+  cudaStream_t st = ix->stream;
+  if (n) {
+    CU(cudaMemcpyAsync(dh.p, hashes, n * 4, cudaMemcpyHostToDevice, st));
+    k_bucket_sizes<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(ix->dix.dir, dh.as<uint32_t>(), dc.as<uint32_t>(), n);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(counts, dc.p, n * 4, cudaMemcpyDeviceToHost, st));
+  }
+  CU(cudaStreamSynchronize(st));
   return MG_OK;
 }
 

@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -265,6 +267,13 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
   if (headers.size() != n_refs) return fail(MHM_ERR_LIMIT, "one header per reference required");
   const uint32_t step = (uint32_t)k / 2;
   const int hlen = k - (int)step + 1;  // Hashmap.cpp:2790
+  const bool trace = std::getenv("MG_BUILD_TRACE") != nullptr;
+  auto t_start = std::chrono::steady_clock::now();
+  auto phase = [&](const char* what) {
+    if (trace)
+      std::fprintf(stderr, "[mhm_build] %-12s %.3f s\n", what,
+                   std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count());
+  };
   std::string nn(hlen, 'N');
   const uint32_t h_nnn = hash28((const uint8_t*)nn.data(), hlen);
   // 1. hash every indexed position of every reference (TBuildHashmapForReference,
@@ -318,6 +327,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
     }
     m += c;
   }
+  phase("hashed");
   // 2. group by hash: partition on the top 20 hash bits, then sort every partition by
   // (hash, position, refID). The reference sorts a bucket by position only with std::sort
   // (Hashmap.cpp:1566), leaving equal positions in an unspecified order; readers treat every
@@ -337,6 +347,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
     parallel_for(m, std::max(1, nthreads), [&](uint64_t lo, uint64_t hi, int) {
       for (uint64_t i = lo; i < hi; i++) pc[ph[i] >> (28 - PB)].fetch_add(1, std::memory_order_relaxed);
     });
+    phase("histogram");
     for (uint64_t p = 0; p < NP; p++) pstart[p + 1] = pstart[p] + pc[p].load(std::memory_order_relaxed);
     for (uint64_t p = 0; p < NP; p++) pc[p].store(pstart[p], std::memory_order_relaxed);
     try {
@@ -351,6 +362,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
       }
     });
   }
+  phase("scattered");
   std::vector<uint32_t>().swap(ph);
   std::vector<uint32_t>().swap(pref);
   std::vector<uint32_t>().swap(ppos);
@@ -358,6 +370,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
     for (uint64_t p = lo; p < hi; p++)
       if (pstart[p + 1] - pstart[p] > 1) std::sort(ent.begin() + pstart[p], ent.begin() + pstart[p + 1]);
   });
+  phase("sorted");
   std::vector<Group> groups;
   uint32_t max_group = 0;
   for (uint64_t i = 0; i < m;) {
@@ -392,6 +405,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
     groups.swap(kept);
   }
   const uint64_t ng = groups.size();
+  phase("grouped");
   // 3. per-record widths and sizes (GetSaveHashmapPreCalculates, Hashmap.cpp:1619-1697)
   std::vector<uint64_t> rec_size(ng);
   std::atomic<int> too_wide(0);
@@ -417,6 +431,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
     }
   });
   if (too_wide) return fail(MHM_ERR_LIMIT, "a bucket has more distinct positions than its width can count");
+  phase("sized");
   // 4. layout and stream positions (SaveHashmapTableV3, Hashmap.cpp:1868-2128)
   uint64_t seq_chars = offs[n_refs] - offs[0], hdr_chars = 0, max_ref = 0, max_hdr = 0;
   for (uint32_t r = 0; r < n_refs; r++) {
@@ -451,11 +466,13 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
   // the 32-bit build refuses files whose positions pass 2^32-1 (Hashmap.cpp:2103-2109)
   if (W == 4 && total - (ng ? rec_size[ng - 1] : 0) > 0xFFFFFFFFull)
     return fail(MHM_ERR_LIMIT, "file too large for the 32-bit format; use word 8");
+  phase("planned");
   try {
     out->assign(total, 0);
   } catch (...) {
     return fail(MHM_ERR_OOM, "out of host memory for the image");
   }
+  phase("allocated");
   uint8_t* b = out->data();
   uint64_t o = 0;
   std::memcpy(b, kMagic, ml);
@@ -518,6 +535,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
     b[o++] = 0;
   }
   if (o != first_rec) return fail(MHM_ERR_FORMAT, "internal layout mismatch");
+  phase("laid out");
   // 5. posting records (Hashmap.cpp:2303-2512)
   parallel_for(ng, std::max(1, nthreads), [&](uint64_t lo, uint64_t hi, int) {
     for (uint64_t g = lo; g < hi; g++) {
@@ -561,6 +579,7 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
       }
     }
   });
+  phase("encoded");
   return MHM_OK;
 }
 

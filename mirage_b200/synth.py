@@ -12,6 +12,8 @@ Workloads (``scale`` shrinks counts, never per-sequence shapes):
               into 300 Mbp +- 10%), GC fraction per reference uniform in [0.3, 0.7];
               1,000,000 reads of uniform length in [75, 300] bp with 0.5% substitutions and
               0.1% single-base indels, 20% unrelated (GC 0.5).
+* ``uneven_fast`` the same shapes with a vectorised read generator and a separate read seed
+              (the benchmark's form: one reference set, one read set per GPU).
 * ``long``    the same references; 100,000 reads, log-normal length (median 5 kb, clipped to
               1-20 kb), 3% substitutions + 2% indels, 10% chimeras of two references.
 * ``repeats`` 20,000 references, log-normal (median 80 kb, sigma 0.67), 5% of every reference
@@ -218,9 +220,71 @@ def _fast_fixed_reads(refs: SeqSet, n_related: int, n_unrelated: int, L: int, rn
     return SeqSet(data, offs, [b"read%d" % i for i in range(n)]), truth
 
 
-def workload(name: str, scale: float = 1.0, seed: int = 1, n_reads: int | None = None):
-    """Return (references, reads, truth) for a named workload."""
+def _fast_variable_reads(refs: SeqSet, n_related: int, n_unrelated: int, lo: int, hi: int, rng, sub: float,
+                         indel: float):
+    """Vectorised reads of uniform length in [lo, hi] with substitutions and single-base
+    indels (half insertions of a uniform base, half deletions), random reference, position and
+    strand; then uniform unrelated reads."""
+    n = n_related + n_unrelated
+    lens = rng.integers(lo, hi + 1, size=n).astype(np.int64)
+    W = hi + 4
+    rlen = refs.lengths().astype(np.int64)
+    ok = np.flatnonzero(rlen >= W + 2)
+    r = ok[rng.integers(0, len(ok), size=n_related)]
+    p = (rng.random(n_related) * (rlen[r] - W + 1)).astype(np.int64)
+    start = refs.offs[r].astype(np.int64) + p
+    mat = refs.data[start[:, None] + np.arange(W)[None, :]]
+    # substitutions over the whole source window (what falls past the read end is dropped)
+    flat = mat.reshape(-1)
+    _substitute(rng, flat, sub)
+    # indels: per read a binomial count; applied row by row only where there are any
+    n_ev = rng.binomial(lens[:n_related], indel)
+    for i in np.flatnonzero(n_ev):
+        row = mat[i]
+        L = int(lens[i])
+        pos = np.sort(rng.integers(0, L, size=int(n_ev[i])))
+        ins = rng.random(len(pos)) < 0.5
+        s = row
+        for q, is_ins in zip(pos[::-1], ins[::-1]):
+            if is_ins:
+                s = np.concatenate([s[:q], ACGT[rng.integers(0, 4, size=1)], s[q:]])
+            else:
+                s = np.concatenate([s[:q], s[q + 1 :]])
+        mat[i] = s[:W] if len(s) >= W else np.concatenate([s, row[len(s) - W :]])[:W]
+    # strand: reverse-complement the read part of half the rows
+    flip = rng.random(n_related) < 0.5
+    fi = np.flatnonzero(flip)
+    if len(fi):
+        Lf = lens[fi]
+        idx = np.clip(Lf[:, None] - 1 - np.arange(W)[None, :], 0, W - 1)
+        mat[fi] = _COMP[np.take_along_axis(mat[fi], idx, axis=1)]
+    valid = np.arange(W)[None, :] < lens[:n_related, None]
+    rel = mat[valid]
+    unrel = ACGT[rng.integers(0, 4, size=int(lens[n_related:].sum())).astype(np.uint8)]
+    data = np.concatenate([rel, unrel])
+    offs = np.zeros(n + 1, dtype=np.uint64)
+    offs[1:] = np.cumsum(lens)
+    truth = np.concatenate([r, np.full(n_unrelated, -1)])
+    return SeqSet(data, offs, [b"read%d" % i for i in range(n)]), truth
+
+
+def workload(name: str, scale: float = 1.0, seed: int = 1, n_reads: int | None = None,
+             reads_seed: int | None = None, refs: SeqSet | None = None):
+    """Return (references, reads, truth) for a named workload. With reads_seed the reads come
+    from their own generator (so several read sets can share one reference set, which `refs`
+    may pass in already generated)."""
     rng = np.random.default_rng(seed)
+    if name == "uneven_fast":
+        n_refs = max(4, int(round(5000 * scale)))
+        if refs is None:
+            total = 344e6 * n_refs / 5000
+            lens = _lognormal_lengths(rng, n_refs, 50_000, 0.8, lo=1000, total=total, tol=0.1)
+            refs = make_references(n_refs, lens, rng.uniform(0.3, 0.7, size=n_refs), rng)
+        rr = np.random.default_rng(reads_seed if reads_seed is not None else seed + 1_000_003)
+        nr = n_reads if n_reads is not None else int(round(1_000_000 * scale))
+        n_unrel = nr // 5
+        reads, truth = _fast_variable_reads(refs, nr - n_unrel, n_unrel, 75, 300, rr, 0.005, 0.001)
+        return refs, reads, truth
     if name == "plain":
         n_refs = max(2, int(round(200 * min(1.0, scale * 4))))
         refs = make_references(n_refs, np.full(n_refs, 5000), np.full(n_refs, 0.5), rng)

@@ -116,6 +116,7 @@ struct Opts {
   int threads = 1;
   bool time_only = false;
   long limit = -1;
+  int repeat = 1;
   int k = 31;
   bool first_only = true;
 };
@@ -143,6 +144,7 @@ int main(int argc, char** argv) {
     else if (a == "--threads") o.threads = std::stoi(next());
     else if (a == "--time") o.time_only = true;
     else if (a == "--limit") o.limit = std::stol(next());
+    else if (a == "--repeat") o.repeat = std::stoi(next());
     else if (a == "--k") o.k = std::stoi(next());
     else if (a == "--all-groups") o.first_only = false;
     else usage();
@@ -205,6 +207,10 @@ int main(int argc, char** argv) {
   }
   size_t nq = qids.size();
 
+  // --time --repeat R: the hot path R times over the same reads (the index stays loaded);
+  // one JSON line per repetition.
+  const int reps = o.time_only ? std::max(1, o.repeat) : 1;
+  for (int rep = 0; rep < reps; rep++) {
   Analyser::Analysis_Arguments* args = new Analyser::Analysis_Arguments();
   args->matchedReferencesPerQuery_CombiPositions_LastPositionInRange.resize(nq);
   args->matchedReferencesPerQuery_HeadTailSequences.resize(nq);
@@ -301,11 +307,14 @@ int main(int argc, char** argv) {
   double load_s = std::chrono::duration<double>(t_load1 - t_load0).count();
   double total = prep_s + score_s + pick_s;
   std::fprintf(stderr,
-               "{\"reads\": %zu, \"job\": %zu, \"threads\": %d, \"load_s\": %.4f, \"prep_s\": %.4f, "
+               "{\"rep\": %d, \"reads\": %zu, \"job\": %zu, \"threads\": %d, \"load_s\": %.4f, \"prep_s\": %.4f, "
                "\"score_s\": %.4f, \"pick_s\": %.4f, \"hot_s\": %.4f, \"reads_per_s\": %.2f}\n",
-               n_reads, job, o.threads, load_s, prep_s, score_s, pick_s, total,
+               rep, n_reads, job, o.threads, load_s, prep_s, score_s, pick_s, total,
                total > 0 ? n_reads / total : 0.0);
-  if (o.time_only) return 0;
+  if (o.time_only) {
+    delete args;
+    continue;
+  }
 
   if (logs) {
     // The reference's own log writer (Analyser.cpp:378-491).
@@ -364,5 +373,6 @@ int main(int argc, char** argv) {
     }
     std::fclose(f);
   }
+  }  // repetitions
   return 0;
 }
