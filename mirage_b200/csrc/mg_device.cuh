@@ -45,7 +45,10 @@ struct BatchDev {
   uint64_t cand_cap;
   unsigned long long* n_cands;   // output cursor
   int* err;                      // OR of kErr* bits
-  unsigned int* work;            // work-stealing cursor for the warp tier
+  unsigned int* work;            // work-stealing cursor for the lean warp tier
+  uint32_t* ovf0;                // reads handed to the general warp tier
+  unsigned int* n_ovf0;
+  unsigned int* work1;           // cursor over ovf0
   uint32_t* ovf1;                // reads handed to the block tier
   unsigned int* n_ovf1;
   unsigned int* work2;           // cursor over ovf1

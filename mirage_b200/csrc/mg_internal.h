@@ -1,0 +1,74 @@
+// Host-side internals shared by the library's translation units (index, pipeline, server).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../include/mirage_b200.h"
+#include "mg_device.cuh"
+#include "mhm.h"
+
+namespace mg {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  int alloc(size_t bytes) {
+    if (bytes <= n && p) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return -1;
+    n = bytes;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T* as() const {
+    return (T*)p;
+  }
+};
+
+// Device buffers of one classification call in flight (a call owns one at a time).
+struct Workspace {
+  DevBuf offs, bases, reads, stage, arena, cands, ctr, ovf, sums, gws;
+  void release() {
+    for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws}) b->release();
+  }
+  size_t bytes() const {
+    return offs.n + bases.n + reads.n + stage.n + arena.n + cands.n + ctr.n + ovf.n + sums.n + gws.n;
+  }
+};
+
+int set_error(int code, const std::string& msg);
+// Size ws for n_reads reads (n_bases bases when host_io: the input and result buffers too).
+int ensure_workspace(Workspace& ws, uint64_t n_reads, uint64_t n_bases, bool host_io);
+// Queue the fused pipeline (warp, block and global tiers, then compaction) on stream st.
+int run_pipeline(mg_index* ix, Workspace& ws, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
+                 mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain);
+// Wait for st, read the error word and the candidate count of the call that used ws.
+int finish_errors(Workspace& ws, cudaStream_t st, uint64_t* n_cands);
+
+}  // namespace mg
+
+struct mg_index {
+  int device = 0;
+  mg::DevIndex dix{};
+  mg::MhmIndex host;  // refs, headers, taxids kept; postings released after upload
+  mg::DevBuf dir, post, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals;
+  mg::Workspace ws;   // workspace of the synchronous entry points
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  mg_index_info info{};
+  uint64_t device_bytes = 0;
+  // optional per-kernel timing of the last pipeline (events on the launching stream)
+  bool timing = false;
+  bool events_made = false;
+  cudaEvent_t ev[5];
+};

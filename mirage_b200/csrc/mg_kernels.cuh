@@ -320,6 +320,44 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
   return kStrandOk;
 }
 
+// Strand merge (Analyser.cpp:592-611), the log skip rule (:388) and the staging write of one
+// read's scored candidates (forward strand first). Called by one thread.
+__device__ __forceinline__ void write_read_result(const BatchDev& b, uint32_t r, bool bad, const uint32_t* n,
+                                                  const float* h, mg_candidate* const* cb, mg_candidate* stage,
+                                                  mg_candidate* arena, uint64_t arena_cap,
+                                                  unsigned long long* arena_n, int* errw, int err) {
+  mg_read_result rr;
+  if (bad) {
+    err |= kErrBadInput;
+    rr = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
+  } else {
+    const int ch = h[0] < h[1] ? 1 : 0;  // Analyser.cpp:601
+    uint32_t top = 0;
+    for (uint32_t c = 0; c < n[ch]; c++) top += cb[ch][c].rel == h[ch];
+    const uint32_t tot = n[0] + n[1];
+    uint32_t where = 0;
+    mg_candidate* dst = stage + (uint64_t)r * kSlots;
+    if (tot > (uint32_t)kSlots) {
+      unsigned long long at = atomicAdd(arena_n, (unsigned long long)tot);
+      if (at + tot > arena_cap) {
+        err |= kErrOutput;
+        dst = nullptr;
+      } else {
+        dst = arena + at;
+        where = (uint32_t)at;
+      }
+    }
+    if (dst) {
+      for (uint32_t c = 0; c < n[0]; c++) dst[c] = cb[0][c];
+      for (uint32_t c = 0; c < n[1]; c++) dst[n[0] + c] = cb[1][c];
+    }
+    const uint8_t reported = (n[ch] > 0 && h[ch] != 0.0f) ? 1 : 0;  // Analyser.cpp:388
+    rr = mg_read_result{h[ch], where, (uint16_t)n[0], (uint16_t)n[1], (uint8_t)ch, reported, (uint16_t)top};
+  }
+  b.reads[r] = rr;
+  if (err) atomicOr(errw, err);
+}
+
 // Both strands of read r, the strand merge and the staging write. Returns false when the
 // read must go to a larger tier.
 template <int G>
@@ -333,44 +371,13 @@ __device__ bool process_read(const DevIndex& ix, const BatchDev& b, uint32_t r, 
   const uint32_t L = (uint32_t)Lr;
   const uint8_t* raw = b.bases + o0;
   int err = 0;
-  uint32_t n[2];
-  float h[2];
+  uint32_t n[2] = {0, 0};
+  float h[2] = {-1.0f, -1.0f};
   int st = process_strand<G>(ix, raw, L, 0, ws, caps, red, &err, &n[0], &h[0]);
   if (st == kStrandOverflow) return false;
   if (st != kStrandBad) st = process_strand<G>(ix, raw, L, 1, ws, caps, red, &err, &n[1], &h[1]);
   if (st == kStrandOverflow) return false;
-  if (tid == 0) {
-    mg_read_result rr;
-    if (st == kStrandBad) {
-      err |= kErrBadInput;
-      rr = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
-    } else {
-      const int ch = h[0] < h[1] ? 1 : 0;  // Analyser.cpp:601
-      uint32_t top = 0;
-      for (uint32_t c = 0; c < n[ch]; c++) top += ws.cb[ch][c].rel == h[ch];
-      const uint32_t tot = n[0] + n[1];
-      uint32_t where = 0;
-      mg_candidate* dst = stage + (uint64_t)r * kSlots;
-      if (tot > (uint32_t)kSlots) {
-        unsigned long long at = atomicAdd(arena_n, (unsigned long long)tot);
-        if (at + tot > arena_cap) {
-          err |= kErrOutput;
-          dst = nullptr;
-        } else {
-          dst = arena + at;
-          where = (uint32_t)at;
-        }
-      }
-      if (dst) {
-        for (uint32_t c = 0; c < n[0]; c++) dst[c] = ws.cb[0][c];
-        for (uint32_t c = 0; c < n[1]; c++) dst[n[0] + c] = ws.cb[1][c];
-      }
-      const uint8_t reported = (n[ch] > 0 && h[ch] != 0.0f) ? 1 : 0;  // Analyser.cpp:388
-      rr = mg_read_result{h[ch], where, (uint16_t)n[0], (uint16_t)n[1], (uint8_t)ch, reported, (uint16_t)top};
-    }
-    b.reads[r] = rr;
-    if (err) atomicOr(errw, err);
-  }
+  if (tid == 0) write_read_result(b, r, st == kStrandBad, n, h, ws.cb, stage, arena, arena_cap, arena_n, errw, err);
   Grp<G>::sync();
   return true;
 }

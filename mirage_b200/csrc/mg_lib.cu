@@ -17,13 +17,14 @@
 #include "../../include/mirage_b200.h"
 #include "mg_device.cuh"
 #include "mg_kernels.cuh"
+#include "mg_lean.cuh"
 #include "mhm.h"
 
 namespace mg {
 
 // ------------------------------------------------------------------------------ errors
 
-static thread_local std::string g_last_error;
+thread_local std::string g_last_error;
 
 int set_error(int code, const std::string& msg) {
   g_last_error = msg;
@@ -108,7 +109,49 @@ struct StageDev {
   unsigned long long* arena_n;
 };
 
+// Lean warp tier: every read of the batch, one warp per read, work stealing in chunks; reads
+// that do not fit the lean path go to the general warp tier.
+struct LeanSmem {
+  uint32_t a[8][kLeanE];
+  mg_candidate cb[2][kW1C];
+  uint8_t q[kLeanQ];
+};
+
 __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp(DevIndex ix, BatchDev b, StageDev sd) {
+  __shared__ LeanSmem sm[kW1Warps];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  LeanSmem& S = sm[w];
+  LeanWS lw;
+  lw.e_ref = S.a[0];
+  lw.e_pos = S.a[1];
+  lw.e_fj = S.a[2];
+  lw.s_ref = S.a[3];
+  lw.s_pos = S.a[4];
+  lw.s_j = S.a[5];
+  lw.z = S.a[6];
+  lw.segmax = S.a[7];
+  mg_candidate* const cbs[2] = {S.cb[0], S.cb[1]};
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((uint64_t)base >= b.n) break;
+    const uint64_t end64 = (uint64_t)base + kW1Chunk;
+    const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
+    for (uint32_t r = base; r < end; r++) {
+      if (!process_read_lean(ix, b, r, S.q, lw, cbs, kW1C, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+        if (lane == 0) {
+          unsigned at = atomicAdd(b.n_ovf0, 1u);
+          b.ovf0[at] = r;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// General warp tier over the lean tier's leftovers; its own leftovers go to the block tier.
+__global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp_list(DevIndex ix, BatchDev b, StageDev sd) {
   __shared__ WarpSmem sm[kW1Warps];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   WarpSmem& S = sm[w];
@@ -122,22 +165,20 @@ __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp(DevIndex ix, Ba
   ws.cb[0] = S.cb[0];
   ws.cb[1] = S.cb[1];
   const Caps caps{kW1Q, kW1Seeds, kW1E, kW1C};
+  const uint32_t n = *b.n_ovf0;
   for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if ((uint64_t)base >= b.n) break;
-    const uint64_t end64 = (uint64_t)base + kW1Chunk;
-    const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
-    for (uint32_t r = base; r < end; r++) {
-      if (!process_read<32>(ix, b, r, ws, caps, &S.red, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
-        if (lane == 0) {
-          unsigned at = atomicAdd(b.n_ovf1, 1u);
-          b.ovf1[at] = r;
-        }
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(b.work1, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= n) break;
+    const uint32_t r = b.ovf0[item];
+    if (!process_read<32>(ix, b, r, ws, caps, &S.red, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+      if (lane == 0) {
+        unsigned at = atomicAdd(b.n_ovf1, 1u);
+        b.ovf1[at] = r;
       }
-      __syncwarp();
     }
+    __syncwarp();
   }
 }
 
@@ -309,47 +350,9 @@ __global__ void k_score_candidates(DevIndex ix, uint64_t n_strands, const uint64
 
 // ------------------------------------------------------------------------------ host side
 
-struct DevBuf {
-  void* p = nullptr;
-  size_t n = 0;
-  int alloc(size_t bytes) {
-    if (bytes <= n && p) return 0;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return -1;
-    n = bytes;
-    return 0;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  template <class T>
-  T* as() const {
-    return (T*)p;
-  }
-};
-
 }  // namespace mg
 
-struct mg_index {
-  int device = 0;
-  mg::DevIndex dix{};
-  mg::MhmIndex host;  // refs, headers, taxids kept; postings released after upload
-  mg::DevBuf dir, post, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals;
-  // per-call workspace
-  mg::DevBuf w_offs, w_bases, w_reads, w_stage, w_arena, w_cands, w_ctr, w_ovf, w_sums, w_gws;
-  cudaStream_t stream = nullptr;
-  std::mutex mu;
-  mg_index_info info{};
-  uint64_t device_bytes = 0;
-  // optional per-kernel timing of the last pipeline (events on the launching stream)
-  bool timing = false;
-  bool events_made = false;
-  cudaEvent_t ev[5];
-};
+#include "mg_internal.h"
 
 namespace mg {
 
@@ -489,28 +492,28 @@ struct Plan {
   bool plain;  // block-per-read form
 };
 
-static int ensure_workspace(mg_index* ix, uint64_t n_reads, uint64_t n_bases, bool host_io) {
+int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host_io) {
   uint64_t arena_cap = std::max<uint64_t>(1 << 16, n_reads * 2);
   if (host_io) {
-    if (ix->w_offs.alloc((n_reads + 1) * 8) || ix->w_bases.alloc(n_bases + 16) ||
-        ix->w_reads.alloc(n_reads * sizeof(mg_read_result) + 16))
+    if (w.offs.alloc((n_reads + 1) * 8) || w.bases.alloc(n_bases + 16) ||
+        w.reads.alloc(n_reads * sizeof(mg_read_result) + 16))
       return set_error(MG_ERR_OOM, "batch buffers");
   }
-  if (ix->w_stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
-      ix->w_arena.alloc(arena_cap * sizeof(mg_candidate)) || ix->w_ctr.alloc(256) ||
-      ix->w_ovf.alloc(2 * n_reads * 4 + 16) || ix->w_sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+  if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
+      w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
+      w.ovf.alloc(3 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
-  if (ix->w_gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
+  if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
   return MG_OK;
 }
 
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
-// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64)
-static int run_pipeline(mg_index* ix, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
+// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1
+int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
                         bool plain) {
-  uint8_t* ctr = ix->w_ctr.as<uint8_t>();
+  uint8_t* ctr = w.ctr.as<uint8_t>();
   CU(cudaMemsetAsync(ctr, 0, 256, st));
   BatchDev b;
   b.n = n;
@@ -526,12 +529,15 @@ static int run_pipeline(mg_index* ix, uint64_t n, const uint64_t* d_offs, const 
   b.work2 = (unsigned*)(ctr + 28);
   b.n_ovf2 = (unsigned*)(ctr + 32);
   b.work3 = (unsigned*)(ctr + 36);
-  b.ovf1 = ix->w_ovf.as<uint32_t>();
-  b.ovf2 = ix->w_ovf.as<uint32_t>() + n + 4;
+  b.n_ovf0 = (unsigned*)(ctr + 48);
+  b.work1 = (unsigned*)(ctr + 52);
+  b.ovf0 = w.ovf.as<uint32_t>();
+  b.ovf1 = w.ovf.as<uint32_t>() + n + 4;
+  b.ovf2 = w.ovf.as<uint32_t>() + 2 * (n + 4);
   StageDev sd;
-  sd.stage = ix->w_stage.as<mg_candidate>();
-  sd.arena = ix->w_arena.as<mg_candidate>();
-  sd.arena_cap = ix->w_arena.n / sizeof(mg_candidate);
+  sd.stage = w.stage.as<mg_candidate>();
+  sd.arena = w.arena.as<mg_candidate>();
+  sd.arena_cap = w.arena.n / sizeof(mg_candidate);
   sd.arena_n = (unsigned long long*)(ctr + 8);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
@@ -557,6 +563,9 @@ static int run_pipeline(mg_index* ix, uint64_t n, const uint64_t* d_offs, const 
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_classify_warp, kW1Warps * 32, 0);
       unsigned grid = (unsigned)std::max(1, per_sm) * sms;
       k_classify_warp<<<grid, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      int per_sm2 = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
+      k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
       k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, st>>>(
           ix->dix, b, sd, b.ovf1, b.n_ovf1, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
@@ -564,11 +573,11 @@ static int run_pipeline(mg_index* ix, uint64_t n, const uint64_t* d_offs, const 
     }
     CU(cudaGetLastError());
     k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, st>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3,
-                                                                   nullptr, nullptr, ix->w_gws.as<uint8_t>(), l3, c3, 1);
+                                                                   nullptr, nullptr, w.gws.as<uint8_t>(), l3, c3, 1);
     if (tm) CU(cudaEventRecord(ix->ev[3], st));
     CU(cudaGetLastError());
     const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
-    unsigned long long* sums = ix->w_sums.as<unsigned long long>();
+    unsigned long long* sums = w.sums.as<unsigned long long>();
     k_count_sums<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums);
     k_scan_sums<<<1, 32, 0, st>>>(sums, nb, (unsigned long long*)(ctr + 40));
     k_scatter<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums, sd, d_out, cap, b.err);
@@ -578,9 +587,9 @@ static int run_pipeline(mg_index* ix, uint64_t n, const uint64_t* d_offs, const 
   return MG_OK;
 }
 
-static int finish_errors(mg_index* ix, cudaStream_t st, uint64_t* n_cands) {
+int finish_errors(Workspace& w, cudaStream_t st, uint64_t* n_cands) {
   uint8_t h[64];
-  CU(cudaMemcpyAsync(h, ix->w_ctr.p, 64, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(h, w.ctr.p, 64, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   int err;
   unsigned long long total;
@@ -603,25 +612,26 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   if (n >= 0xFFFFFFF0ull) return set_error(MG_ERR_LIMIT, "too many reads in one batch");
   const uint64_t nb = n ? batch->offsets[n] : 0;
   if (n && batch->offsets[0] != 0) return set_error(MG_ERR_INVAL, "offsets[0] must be 0");
-  int rc = ensure_workspace(ix, n, nb, true);
+  Workspace& w = ix->ws;
+  int rc = ensure_workspace(w, n, nb, true);
   if (rc) return rc;
-  if (ix->w_cands.alloc(std::max<uint64_t>(out->cand_cap, 1) * sizeof(mg_candidate)))
+  if (w.cands.alloc(std::max<uint64_t>(out->cand_cap, 1) * sizeof(mg_candidate)))
     return set_error(MG_ERR_OOM, "candidate buffer");
   cudaStream_t st = ix->stream;
   if (n) {
-    CU(cudaMemcpyAsync(ix->w_offs.p, batch->offsets, (n + 1) * 8, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(ix->w_bases.p, batch->bases, nb, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(w.offs.p, batch->offsets, (n + 1) * 8, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(w.bases.p, batch->bases, nb, cudaMemcpyHostToDevice, st));
   }
-  rc = run_pipeline(ix, n, ix->w_offs.as<uint64_t>(), ix->w_bases.as<uint8_t>(), ix->w_reads.as<mg_read_result>(),
-                    ix->w_cands.as<mg_candidate>(), out->cand_cap, st, plain);
+  rc = run_pipeline(ix, w, n, w.offs.as<uint64_t>(), w.bases.as<uint8_t>(), w.reads.as<mg_read_result>(),
+                    w.cands.as<mg_candidate>(), out->cand_cap, st, plain);
   if (rc) return rc;
   uint64_t total = 0;
-  rc = finish_errors(ix, st, &total);
+  rc = finish_errors(w, st, &total);
   out->n_cands = total;
   if (rc) return rc;
   if (n) {
-    CU(cudaMemcpyAsync(out->reads, ix->w_reads.p, n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, st));
-    if (total) CU(cudaMemcpyAsync(out->cands, ix->w_cands.p, total * sizeof(mg_candidate), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(out->reads, w.reads.p, n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, st));
+    if (total) CU(cudaMemcpyAsync(out->cands, w.cands.p, total * sizeof(mg_candidate), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
   }
   return MG_OK;
@@ -693,9 +703,9 @@ void mg_close(mg_index* ix) {
   if (!ix) return;
   cudaSetDevice(ix->device);
   for (DevBuf* b : {&ix->dir, &ix->post, &ix->bases, &ix->ref_off, &ix->ref_len, &ix->logx_bitmap, &ix->logx_keys,
-                    &ix->logx_vals, &ix->w_offs, &ix->w_bases, &ix->w_reads, &ix->w_stage, &ix->w_arena,
-                    &ix->w_cands, &ix->w_ctr, &ix->w_ovf, &ix->w_sums, &ix->w_gws})
+                    &ix->logx_vals})
     b->release();
+  ix->ws.release();
   if (ix->stream) cudaStreamDestroy(ix->stream);
   if (ix->events_made)
     for (auto& e : ix->ev) cudaEventDestroy(e);
@@ -827,19 +837,20 @@ int mg_classify_device(mg_index* ix, uint64_t n, const uint64_t* d_offs, const u
   if (!ix || (n && (!d_offs || !d_bases || !d_reads))) return set_error(MG_ERR_INVAL, "null argument");
   std::lock_guard<std::mutex> lk(ix->mu);
   CU(cudaSetDevice(ix->device));
-  int rc = ensure_workspace(ix, n, 0, false);
+  Workspace& w = ix->ws;
+  int rc = ensure_workspace(w, n, 0, false);
   if (rc) return rc;
   cudaStream_t st = stream ? (cudaStream_t)stream : ix->stream;
-  rc = run_pipeline(ix, n, d_offs, d_bases, d_reads, d_cands, cand_cap, st, false);
+  rc = run_pipeline(ix, w, n, d_offs, d_bases, d_reads, d_cands, cand_cap, st, false);
   if (rc) return rc;
-  if (d_n_cands) CU(cudaMemcpyAsync(d_n_cands, ix->w_ctr.as<uint8_t>() + 40, 8, cudaMemcpyDeviceToDevice, st));
+  if (d_n_cands) CU(cudaMemcpyAsync(d_n_cands, w.ctr.as<uint8_t>() + 40, 8, cudaMemcpyDeviceToDevice, st));
   return MG_OK;
 }
 
 int mg_classify_device_sync(mg_index* ix, void* stream, uint64_t* n_cands) {
   if (!ix || !n_cands) return set_error(MG_ERR_INVAL, "null argument");
   cudaStream_t st = stream ? (cudaStream_t)stream : ix->stream;
-  return finish_errors(ix, st, n_cands);
+  return finish_errors(ix->ws, st, n_cands);
 }
 
 int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off, const uint8_t* bases,
