@@ -60,11 +60,22 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
         return self
+
+    def wait_first(self, timeout: float = 5.0) -> None:
+        """Block until nvidia-smi has written its first sample (or the timeout passes)."""
+        t = time.time()
+        while self.proc and time.time() - t < timeout:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    return
+            except OSError:
+                pass
+            time.sleep(0.05)
 
     def __exit__(self, *exc):
         if self.proc:
@@ -234,7 +245,7 @@ def run_reference_arm(args, rank: int, world: int) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mirage", choices=["mirage", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the reference set (tests)")
@@ -316,44 +327,45 @@ def main():
         return float(t.item())
 
     ix.set_timing(True)
-    for _ in range(args.warmup):
-        device_step()
-        ix.device_sync(sp)
-    barrier()
     kernel_ms = np.zeros(4)
     step_ms = []
+    # the clock sampler runs from before the warm-up to the end of the e2e timed region
     with ClockSampler(local) as clk:
+        clk.wait_first()
+        for _ in range(args.warmup):
+            device_step()
+            ix.device_sync(sp)
+        barrier()
         start = torch.cuda.Event(enable_timing=True)
         end = torch.cuda.Event(enable_timing=True)
         barrier()
-        with torch.cuda.stream(stream):
-            start.record(stream)
+        start.record(stream)
         for _ in range(args.steps):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             device_step()
             e1.record(stream)
-            n_cands = ix.device_sync(sp)
+            n_cands = ix.device_sync(sp)  # per-step error check, as a caller would
             kernel_ms += ix.last_kernel_times()
             step_ms.append(e0.elapsed_time(e1))
         end.record(stream)
         barrier()
         total_ms = start.elapsed_time(end)
-    total_ms = max_over_ranks(total_ms)
-    ms_per_step = total_ms / args.steps
-    value = world * n / (ms_per_step / 1000)
+        total_ms = max_over_ranks(total_ms)
+        ms_per_step = total_ms / args.steps
+        value = world * n / (ms_per_step / 1000)
 
-    # end to end through the C ABI with pinned host buffers
-    for _ in range(args.warmup):
-        e2e_step()
-    barrier()
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        n_c = e2e_step()
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t) / args.steps
-    e2e = world * n / e2e_s
+        # end to end through the C ABI with pinned host buffers
+        for _ in range(args.warmup):
+            e2e_step()
+        barrier()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            n_c = e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t) / args.steps
+        e2e = world * n / e2e_s
     h2d = n_bases + 8 * (n + 1)
     d2h = 16 * n + 16 * n_c + 64
 

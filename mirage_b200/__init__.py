@@ -302,7 +302,7 @@ class Server:
         return t.value
 
     def _result(self, ticket: int, fn, *extra):
-        n = self._pending[ticket][0]
+        n = self._pending[ticket][0] if ticket in self._pending else 0
         cap = max(1024, 8 * n)
         while True:
             reads = np.zeros(n, dtype=READ_DTYPE)
@@ -315,7 +315,7 @@ class Server:
             _check(rc, "mg_server_poll")
             if rc == 0:
                 return None
-            del self._pending[ticket]
+            self._pending.pop(ticket, None)
             return Results(reads, cands[: r.n_cands].copy())
 
     def poll(self, ticket: int) -> Results | None:
