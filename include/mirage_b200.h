@@ -178,6 +178,26 @@ int mg_server_poll(mg_server* s, uint64_t ticket, mg_result* out);
 int mg_server_wait(mg_server* s, uint64_t ticket, mg_result* out, uint32_t timeout_ms);
 void mg_server_destroy(mg_server* s);
 
+/* Result logs in the reference's format (host only). Replaces LogManager::Open +
+ * WriteOutputHeaders (LogManager.cpp:319-404) and Analyser::LogMatrixResults /
+ * LogMatrixResult / LogResultsToFileManager (Analyser.cpp:378-491, 228-376): the four files
+ * results_{HighSensitivity,HighPrecision,Balanced,Raw}.log in out_dir with their headers;
+ * thresholds are the LogThreshold_* settings. mg_logs_write logs n merged results: the
+ * caller's input IDs (InputID column), input headers (with '>', no line end), and per
+ * reference its header (with '>') and TaxID; first_group_only = output_firstresults_only. */
+typedef struct mg_logs mg_logs;
+int mg_logs_open(const char* out_dir, int high_precision_enabled, float th_sensitivity, float th_balanced,
+                 float th_precision, mg_logs** out);
+int mg_logs_write(mg_logs* logs, const mg_read_result* reads, const mg_candidate* cands, uint64_t n,
+                  const uint64_t* input_ids, const char* const* input_headers, const char* const* ref_headers,
+                  const int32_t* taxids, int first_group_only);
+void mg_logs_close(mg_logs* logs);
+/* LogManager::CreateUniqueOutputFolders (LogManager.cpp:288): creates
+ * <output_path>/results_<seconds since epoch> and returns its path in out. */
+int mg_make_results_dir(const char* output_path, char* out, uint64_t out_len);
+/* Header (with '>'), NCBI TaxID and length of reference `ref` of an open index. */
+int mg_index_reference(const mg_index* ix, uint32_t ref, const char** header, int32_t* taxid, uint32_t* length);
+
 const char* mg_strerror(int code);
 const char* mg_last_error(void);
 

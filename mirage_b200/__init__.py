@@ -28,7 +28,8 @@ EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_insp
            "mg_build_image", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_server_create", "mg_server_submit", "mg_server_poll",
-           "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error"]
+           "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error", "mg_logs_open", "mg_logs_write",
+           "mg_logs_close", "mg_make_results_dir", "mg_index_reference"]
 
 
 class MirageError(RuntimeError):
@@ -91,6 +92,13 @@ def lib() -> C.CDLL:
         L.mg_bucket_sizes.argtypes = [vp, vp, vp, u64]
         L.mg_inspect_image.argtypes = [vp, u64, i32, C.POINTER(_Info)]
         L.mg_eval_logf.argtypes = [vp, vp, vp, u64]
+        L.mg_logs_open.argtypes = [C.c_char_p, i32, C.c_float, C.c_float, C.c_float, C.POINTER(vp)]
+        L.mg_logs_write.argtypes = [vp, vp, vp, u64, vp, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p), vp, i32]
+        L.mg_logs_close.argtypes = [vp]
+        L.mg_logs_close.restype = None
+        L.mg_make_results_dir.argtypes = [C.c_char_p, C.c_char_p, u64]
+        L.mg_index_reference.argtypes = [vp, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_uint32)]
         L.mg_strerror.argtypes = [i32]
         L.mg_strerror.restype = C.c_char_p
         L.mg_last_error.restype = C.c_char_p
@@ -136,6 +144,28 @@ def inspect_image(image, k: int = 31) -> dict:
     inf = _Info()
     _check(lib().mg_inspect_image(img.ctypes.data, len(img), k, C.byref(inf)), "mg_inspect_image")
     return {f: getattr(inf, f) for f, _ in _Info._fields_}
+
+
+def write_logs(out_dir: str, results: "Results", input_ids, input_headers, ref_headers, taxids,
+               first_group_only: bool = True, thresholds=(0.4, 0.7, 1.0), high_precision: bool = True) -> None:
+    """Append results to the reference-format logs in out_dir (created with their headers when
+    this call opens them). Headers are bytes including '>'."""
+    L = lib()
+    h = C.c_void_p()
+    _check(L.mg_logs_open(os.fspath(out_dir).encode(), 1 if high_precision else 0, thresholds[0], thresholds[1],
+                          thresholds[2], C.byref(h)), "mg_logs_open")
+    try:
+        n = len(results.reads)
+        ids = np.ascontiguousarray(input_ids, dtype=np.uint64)
+        ih = (C.c_char_p * max(1, n))(*input_headers)
+        rh = (C.c_char_p * max(1, len(ref_headers)))(*ref_headers)
+        tx = np.ascontiguousarray(taxids, dtype=np.int32)
+        reads = np.ascontiguousarray(results.reads)
+        cands = np.ascontiguousarray(results.cands) if len(results.cands) else np.zeros(1, CAND_DTYPE)
+        _check(L.mg_logs_write(h, reads.ctypes.data, cands.ctypes.data, n, ids.ctypes.data, ih, rh, tx.ctypes.data,
+                               1 if first_group_only else 0), "mg_logs_write")
+    finally:
+        L.mg_logs_close(h)
 
 
 class Results:
