@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the MirAge classification hot path on B200.
 
-Workload ("uneven", the BASELINE config that fits one GPU): 5,000 synthetic references with
+Workload ("uneven", the largest configuration quoted that fits one GPU): 5,000 synthetic references with
 log-normal lengths (median 50 kb, sigma 0.8, ~344 Mbp, GC per reference uniform in [0.3, 0.7]),
 1,000,000 reads per GPU of uniform length 75-300 bp with 0.5% substitutions, 0.1% single-base
 indels and 20% unrelated reads; seeded synthetic data (no public read set is named). A step is
@@ -14,6 +14,9 @@ flush is needed between steps.
   e2e         reads/s through the C ABI (mg_classify) from pinned host buffers: host->device
               copy of the reads and device->host copy of every result inside the timed region.
   plain       the same e2e measurement of the plain form (mg_score_batch, one block per read).
+  served      the served form (mg_server_*): saturated reads/s with requests of log-uniform
+              size in [1, 50000] reads, then p50/p99 request latency under Poisson arrivals at
+              25/50/75/90% of that rate.
   roofline    the warp-tier kernel (dominant): algorithmic bytes per launch / its CUDA-event time,
               against the measured HBM copy bandwidth.
   cpu_baseline the reference's own CPU path (oracle/_ref harness) when built, else the CPU
@@ -40,6 +43,9 @@ sys.path.insert(0, ROOT)
 
 SEED = 2024
 N_READS = 1_000_000
+# kernels one batched call launches: warp tier (lean), warp tier (general), block tier, global
+# tier, candidate count, scan, scatter
+LAUNCHES_PER_BATCH = 7
 
 
 def log(*a):
@@ -242,6 +248,99 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s: float, fracs=(0.25, 0.5, 0.75, 0.9)):
+    """Served form (mg_server_*): saturated throughput, then latency under Poisson arrivals at
+    fractions of it. Requests are contiguous slices of the host reads with log-uniform sizes in
+    [1, 50000] reads; each submit copies its request from host memory, each wait returns it."""
+    import collections
+
+    rng = np.random.default_rng(seed)
+    n = len(offs) - 1
+    max_req = min(50000, n)
+
+    def draw():
+        size = int(np.exp(rng.uniform(0.0, np.log(max_req + 1))))
+        size = max(1, min(size, max_req))
+        st = int(rng.integers(0, n - size + 1))
+        return st, size
+
+    def request(st, size):
+        o = offs[st:st + size + 1]
+        return bases[int(o[0]):int(o[-1])], o - o[0]
+
+    sv = M.Server(ix)
+    try:
+        for _ in range(8):  # warm-up
+            sv.wait(sv.submit(*request(*draw())))
+        # saturated: keep the server full for ~level_s seconds
+        q, total, t0 = collections.deque(), 0, time.perf_counter()
+        while time.perf_counter() - t0 < level_s:
+            st, size = draw()
+            b, o = request(st, size)
+            t = sv.submit(b, o)
+            while t is None:
+                sv.wait(q.popleft())
+                t = sv.submit(b, o)
+            q.append(t)
+            total += size
+        while q:
+            sv.wait(q.popleft())
+        sat = total / (time.perf_counter() - t0)
+        mean_size = (max_req - 1) / np.log(max_req) if max_req > 1 else 1.0
+        levels = []
+        for f in fracs:
+            rate = f * sat / mean_size  # requests per second
+            pending = collections.deque()
+            lat, done_reads = [], [0]
+            cv = threading.Condition()
+            finished = [False]
+
+            def waiter():
+                while True:
+                    with cv:
+                        while not pending and not finished[0]:
+                            cv.wait()
+                        if not pending:
+                            return
+                        t, arrive, size = pending.popleft()
+                    sv.wait(t)
+                    lat.append(time.perf_counter() - arrive)
+                    done_reads[0] += size
+
+            th = threading.Thread(target=waiter)
+            th.start()
+            t0 = time.perf_counter()
+            arrive = t0
+            while arrive - t0 < level_s:
+                arrive += rng.exponential(1.0 / rate)
+                now = time.perf_counter()
+                if arrive > now:
+                    time.sleep(arrive - now)
+                st, size = draw()
+                b, o = request(st, size)
+                t = sv.submit(b, o)
+                while t is None:  # admission refused: the wait counts toward latency
+                    time.sleep(5e-5)
+                    t = sv.submit(b, o)
+                with cv:
+                    pending.append((t, arrive, size))
+                    cv.notify()
+            with cv:
+                finished[0] = True
+                cv.notify()
+            th.join()
+            span = time.perf_counter() - t0
+            ms = np.array(lat) * 1000
+            levels.append({"offered_frac": f, "offered_reads_s": f * sat, "achieved_reads_s": done_reads[0] / span,
+                           "requests": len(lat), "p50_ms": float(np.percentile(ms, 50)),
+                           "p99_ms": float(np.percentile(ms, 99))})
+        return {"saturated": {"value": sat, "unit": "reads/s"},
+                "requests": "log-uniform 1..%d reads, contiguous slices of the batch" % max_req,
+                "arrivals": "Poisson", "seconds_per_level": level_s, "load": levels}
+    finally:
+        sv.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -253,6 +352,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=100_000)
     ap.add_argument("--ref-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--served-seconds", type=float, default=3.0, help="seconds per served-form load level (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -381,6 +481,22 @@ def main():
     plain_s = max_over_ranks(time.perf_counter() - t) / plain_steps
     plain = world * n / plain_s
 
+    served = None
+    if args.served_seconds > 0:
+        served = served_bench(M, ix, reads.data, reads.offs, SEED + 100 + rank, args.served_seconds)
+        if dist:  # replicas: throughput adds up, latency is the worst rank's
+            t = torch.tensor([served["saturated"]["value"]] + [x for l in served["load"] for x in
+                              (l["achieved_reads_s"], l["p50_ms"], l["p99_ms"])], dtype=torch.float64,
+                             device=f"cuda:{local}")
+            s = t.clone()
+            dist.all_reduce(s, op=dist.ReduceOp.SUM)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            served["saturated"]["value"] = float(s[0])
+            for i, l in enumerate(served["load"]):
+                l["achieved_reads_s"] = float(s[1 + 3 * i])
+                l["p50_ms"], l["p99_ms"] = float(t[2 + 3 * i]), float(t[3 + 3 * i])
+        served["served_over_plain"] = served["saturated"]["value"] / plain
+
     line = None
     if rank == 0:
         peaks = measured_peaks()
@@ -412,11 +528,12 @@ def main():
                 "plain": {"value": plain, "unit": "reads/s", "ms_per_step": 1000 * plain_s,
                           "what": "mg_score_batch e2e (one block per read, one launch per batch)"},
                 "batched_over_plain_e2e": e2e / plain,
+                "served": served,
                 "kernel_ms_per_step": {"warp_tier": warp_ms, "block_tier": kernel_ms[1] / args.steps,
                                        "global_tier": kernel_ms[2] / args.steps,
                                        "compaction": kernel_ms[3] / args.steps},
                 "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
-                "gpu_launches": args.steps * 6,
+                "gpu_launches": args.steps * LAUNCHES_PER_BATCH,
                 "setup_s": {"generate": t_gen, "index_build": t_build, "open": t_open}}
         print(json.dumps(line), flush=True)
     ix.close()

@@ -60,10 +60,14 @@ typedef struct {
   uint32_t cand_off;   /* first scored candidate of this read in mg_result.cands */
   uint16_t n_fwd;      /* scored candidates of the forward strand (they come first) */
   uint16_t n_rc;       /* scored candidates of the reverse-complement strand */
-  uint8_t strand;      /* 0: forward kept, 1: reverse complement kept */
+  uint8_t strand;      /* 0: forward kept, 1: reverse complement kept; a rejected read holds
+                        * MG_READ_BAD_BYTE or MG_READ_TOO_LARGE (and the call fails) */
   uint8_t reported;    /* 1 when the reference logs this read (Analyser.cpp:388) */
   uint16_t n_top;      /* size of the top-scoring reference group */
 } mg_read_result;
+
+#define MG_READ_BAD_BYTE 0xFF   /* the read holds a byte without a reverse complement */
+#define MG_READ_TOO_LARGE 0xFE  /* the read exceeds the largest workspace tier */
 
 /* One scored candidate (a MatrixResult::ResultsScores entry with its raw score). Candidates
  * of a strand are in ascending refID order, as CreateResultsScores emits them. */
@@ -146,7 +150,9 @@ int mg_classify_device(mg_index* ix, uint64_t n_reads, const uint64_t* d_offsets
                        const uint8_t* d_bases, mg_read_result* d_reads, mg_candidate* d_cands,
                        uint64_t cand_cap, uint64_t* d_n_cands, void* stream);
 /* Waits for work queued by mg_classify_device on `stream` and reports its errors; *n_cands
- * receives the number of candidates written. */
+ * receives the number of candidates written. It completes the index's last mg_classify_device
+ * launch, whose device buffers must stay valid until it returns: a batch whose reads have more
+ * candidates than the internal staging area held is run again here with a larger one. */
 int mg_classify_device_sync(mg_index* ix, void* stream, uint64_t* n_cands);
 
 /* Scoring-only drop-in for MatrixCPU::CPUGetHighestScore (MatrixCPU.cpp:417) when the

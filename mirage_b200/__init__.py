@@ -316,7 +316,7 @@ class Server:
         h = C.c_void_p()
         _check(lib().mg_server_create(index.h, C.byref(cfg), C.byref(h)), "mg_server_create")
         self.h = h
-        self._pending: dict[int, tuple[int, np.ndarray, np.ndarray]] = {}
+        self._pending: dict[int, int] = {}
 
     def submit(self, bases, offsets) -> int | None:
         """Submit a request; returns its ticket, or None when it cannot be admitted now."""
@@ -328,11 +328,11 @@ class Server:
         if rc == -9:
             return None
         _check(rc, "mg_server_submit")
-        self._pending[t.value] = (n, bases, offsets)
+        self._pending[t.value] = n
         return t.value
 
     def _result(self, ticket: int, fn, *extra):
-        n = self._pending[ticket][0] if ticket in self._pending else 0
+        n = self._pending.get(ticket, 0)
         cap = max(1024, 8 * n)
         while True:
             reads = np.zeros(n, dtype=READ_DTYPE)
@@ -342,6 +342,8 @@ class Server:
             if rc == -3 and r.n_cands > cap:
                 cap = int(r.n_cands)
                 continue
+            if rc < 0 and rc != -8:
+                self._pending.pop(ticket, None)  # the server no longer tracks a failed request
             _check(rc, "mg_server_poll")
             if rc == 0:
                 return None

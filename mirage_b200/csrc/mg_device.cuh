@@ -34,6 +34,7 @@ enum : int {
   kErrLimit = 2,      // read beyond every tier's capacity
   kErrOutput = 4,     // candidate buffer too small
   kErrLogRange = 8,   // relative-score log outside the patched domain
+  kErrArena = 16,     // staging arena too small for the reads with more than kSlots candidates
 };
 
 struct BatchDev {

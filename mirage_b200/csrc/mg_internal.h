@@ -54,6 +54,21 @@ int run_pipeline(mg_index* ix, Workspace& ws, uint64_t n, const uint64_t* d_offs
                  mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain);
 // Wait for st, read the error word and the candidate count of the call that used ws.
 int finish_errors(Workspace& ws, cudaStream_t st, uint64_t* n_cands);
+// The pipeline's counters after the stream drains.
+struct Counters {
+  uint64_t n_cands = 0;     // candidates of the batch (written when they fit the output)
+  uint64_t arena_need = 0;  // staging arena entries the batch asked for
+  int err = 0;              // error bits
+  bool reran = false;       // the batch ran again with a larger staging arena
+};
+int read_counters(Workspace& ws, cudaStream_t st, Counters* c);
+// Waits for a launched pipeline and, when the staging arena was too small, grows it to what the
+// kernels asked for and runs the batch again (same arguments as the launch).
+int complete_pipeline(mg_index* ix, Workspace& ws, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
+                      mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain,
+                      Counters* c);
+// Status of error bits as finish_errors reports them.
+int error_status(int err_bits);
 
 }  // namespace mg
 
@@ -71,4 +86,13 @@ struct mg_index {
   bool timing = false;
   bool events_made = false;
   cudaEvent_t ev[5];
+  // arguments of the last mg_classify_device launch, for its completion in the sync call
+  struct {
+    uint64_t n = 0, cap = 0;
+    const uint64_t* offs = nullptr;
+    const uint8_t* bases = nullptr;
+    mg_read_result* reads = nullptr;
+    mg_candidate* cands = nullptr;
+    uint64_t* d_n_cands = nullptr;
+  } last;
 };

@@ -329,7 +329,7 @@ __device__ __forceinline__ void write_read_result(const BatchDev& b, uint32_t r,
   mg_read_result rr;
   if (bad) {
     err |= kErrBadInput;
-    rr = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
+    rr = mg_read_result{-1.0f, 0, 0, 0, MG_READ_BAD_BYTE, 0, 0};
   } else {
     const int ch = h[0] < h[1] ? 1 : 0;  // Analyser.cpp:601
     uint32_t top = 0;
@@ -340,7 +340,7 @@ __device__ __forceinline__ void write_read_result(const BatchDev& b, uint32_t r,
     if (tot > (uint32_t)kSlots) {
       unsigned long long at = atomicAdd(arena_n, (unsigned long long)tot);
       if (at + tot > arena_cap) {
-        err |= kErrOutput;
+        err |= kErrArena;
         dst = nullptr;
       } else {
         dst = arena + at;

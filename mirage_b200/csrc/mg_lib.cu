@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(G) k_classify_block(DevIndex ix, BatchDev b, S
       if (threadIdx.x == 0) {
         if (last_tier) {
           atomicOr(b.err, kErrLimit);
-          b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
+          b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, MG_READ_TOO_LARGE, 0, 0};
         } else {
           unsigned at = atomicAdd(next_n, 1u);
           next[at] = r;
@@ -587,19 +587,44 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   return MG_OK;
 }
 
-int finish_errors(Workspace& w, cudaStream_t st, uint64_t* n_cands) {
+int read_counters(Workspace& w, cudaStream_t st, Counters* c) {
   uint8_t h[64];
   CU(cudaMemcpyAsync(h, w.ctr.p, 64, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
-  int err;
-  unsigned long long total;
-  std::memcpy(&err, h + 16, 4);
+  unsigned long long total, need;
+  std::memcpy(&c->err, h + 16, 4);
+  std::memcpy(&need, h + 8, 8);
   std::memcpy(&total, h + 40, 8);
-  *n_cands = total;
+  c->n_cands = total;
+  c->arena_need = need;
+  return MG_OK;
+}
+
+int complete_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
+                      mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain,
+                      Counters* c) {
+  int rc = read_counters(w, st, c);
+  if (rc || !(c->err & kErrArena)) return rc;
+  if (w.arena.alloc((c->arena_need + (c->arena_need >> 3) + 1024) * sizeof(mg_candidate)))
+    return set_error(MG_ERR_OOM, "staging arena");
+  rc = run_pipeline(ix, w, n, d_offs, d_bases, d_reads, d_out, cap, st, plain);
+  c->reran = true;
+  return rc ? rc : read_counters(w, st, c);
+}
+
+int finish_errors(Workspace& w, cudaStream_t st, uint64_t* n_cands) {
+  Counters c;
+  const int rc = read_counters(w, st, &c);
+  *n_cands = c.n_cands;
+  return rc ? rc : error_status(c.err);
+}
+
+int error_status(int err) {
   if (err & kErrBadInput) return set_error(MG_ERR_BADINPUT, "a read holds a byte without a reverse complement");
   if (err & kErrLimit) return set_error(MG_ERR_LIMIT, "a read exceeds the largest workspace tier");
   if (err & kErrOutput) return set_error(MG_ERR_OOM, "candidate output buffer too small");
   if (err & kErrLogRange) return set_error(MG_ERR_LIMIT, "relative-score logarithm outside its exact domain");
+  if (err & kErrArena) return set_error(MG_ERR_OOM, "staging arena too small");
   return MG_OK;
 }
 
@@ -625,9 +650,13 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   rc = run_pipeline(ix, w, n, w.offs.as<uint64_t>(), w.bases.as<uint8_t>(), w.reads.as<mg_read_result>(),
                     w.cands.as<mg_candidate>(), out->cand_cap, st, plain);
   if (rc) return rc;
-  uint64_t total = 0;
-  rc = finish_errors(w, st, &total);
+  Counters c;
+  rc = complete_pipeline(ix, w, n, w.offs.as<uint64_t>(), w.bases.as<uint8_t>(), w.reads.as<mg_read_result>(),
+                         w.cands.as<mg_candidate>(), out->cand_cap, st, plain, &c);
+  const uint64_t total = c.n_cands;
   out->n_cands = total;
+  if (rc) return rc;
+  rc = error_status(c.err);
   if (rc) return rc;
   if (n) {
     CU(cudaMemcpyAsync(out->reads, w.reads.p, n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, st));
@@ -844,13 +873,25 @@ int mg_classify_device(mg_index* ix, uint64_t n, const uint64_t* d_offs, const u
   rc = run_pipeline(ix, w, n, d_offs, d_bases, d_reads, d_cands, cand_cap, st, false);
   if (rc) return rc;
   if (d_n_cands) CU(cudaMemcpyAsync(d_n_cands, w.ctr.as<uint8_t>() + 40, 8, cudaMemcpyDeviceToDevice, st));
+  ix->last.n = n;
+  ix->last.cap = cand_cap;
+  ix->last.offs = d_offs;
+  ix->last.bases = d_bases;
+  ix->last.reads = d_reads;
+  ix->last.cands = d_cands;
+  ix->last.d_n_cands = d_n_cands;
   return MG_OK;
 }
 
 int mg_classify_device_sync(mg_index* ix, void* stream, uint64_t* n_cands) {
   if (!ix || !n_cands) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
   cudaStream_t st = stream ? (cudaStream_t)stream : ix->stream;
-  return finish_errors(ix->ws, st, n_cands);
+  Counters c;
+  const auto& a = ix->last;
+  int rc = complete_pipeline(ix, ix->ws, a.n, a.offs, a.bases, a.reads, a.cands, a.cap, st, false, &c);
+  *n_cands = c.n_cands;
+  return rc ? rc : error_status(c.err);
 }
 
 int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off, const uint8_t* bases,

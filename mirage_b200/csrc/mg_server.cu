@@ -1,16 +1,14 @@
 // Served form: continuous batching of classification requests against an HBM-resident index.
 //
-// Requests are copied on submit and queued. A server thread forms "steps": it takes reads from
-// the queued requests in arrival order (a request larger than a step spans several steps, and
-// one step carries reads of many requests) and runs the fused pipeline on them. Two step slots
-// each own a device workspace, pinned host staging buffers and a stream, so the next step's
-// copies and kernels run while the previous step's results are drained. A request that arrives
-// while steps are on the device joins the next step formed. Every read is classified
-// independently, so its result is the same alone and in any mix.
-//
-// Admission: a request is refused with MG_ERR_BUSY (retry later) when the tracked request
-// count or the bytes of queued-but-unfinished reads would pass their limits; the step size is
-// fixed at creation from the device memory available.
+// Submit copies a request's reads once, into a pinned host ring shared by all requests; the
+// ring is the admission budget (MG_ERR_BUSY when a request does not fit now, MG_ERR_LIMIT when
+// it can never fit). A server thread forms "steps" from the queued reads in arrival order (a
+// large request spans several steps, one step carries reads of many requests) and runs the
+// fused pipeline on them; each request segment of a step is one host->device copy straight from
+// the ring. Two step slots, each with its own device workspace and stream, let the next step's
+// copies and kernels run while the previous step's results are drained. A request arriving
+// while steps are on the device joins the next step formed. Each read is classified on its
+// own, so a request's results are the same alone and in any mix.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,20 +24,23 @@
 #include <vector>
 
 #include "mg_internal.h"
+#include "mg_ring.h"
 
 namespace mg {
 
 struct Request {
   uint64_t ticket = 0;
   uint64_t n = 0;
-  std::vector<uint64_t> offs;
-  std::vector<uint8_t> bases;
+  uint64_t* offs = nullptr;   // in the pinned ring: n + 1 offsets
+  uint8_t* bases = nullptr;   // in the pinned ring
+  uint64_t ring_at = 0;
   uint64_t next = 0;  // next read to schedule
   uint64_t done = 0;  // reads with results
   std::vector<mg_read_result> reads;
   std::vector<mg_candidate> cands;
   int error = 0;
   bool complete = false;
+  bool released = false;  // ring space returned
 };
 
 struct Part {
@@ -51,26 +52,14 @@ struct Slot {
   Workspace ws;
   cudaStream_t st = nullptr;
   uint64_t* h_offs = nullptr;
-  uint8_t* h_bases = nullptr;
   mg_read_result* h_reads = nullptr;
   mg_candidate* h_cands = nullptr;
-  uint64_t cap_reads = 0, cap_bases = 0, cap_cands = 0;
+  uint64_t cap_reads = 0, cap_cands = 0;
   std::vector<Part> parts;
   uint64_t n = 0;
   bool busy = false;
   int launch_rc = 0;
 };
-
-static bool has_complement(uint8_t c) {
-  const uint8_t u = ((int8_t)c > 96) ? (uint8_t)(c - 32) : c;  // Sequences.cpp:43-55
-  switch (u) {
-    case 'A': case 'T': case 'U': case 'G': case 'C': case 'Y': case 'R': case 'S': case 'W':
-    case 'K': case 'M': case 'B': case 'D': case 'H': case 'V': case 'N': case '-': case '~':
-      return true;
-    default:
-      return false;
-  }
-}
 
 }  // namespace mg
 
@@ -78,11 +67,10 @@ struct mg_server {
   mg_index* ix = nullptr;
   uint64_t step_reads = 0, step_bases = 0;
   uint32_t max_requests = 0;
-  uint64_t queue_budget = 0;   // bytes of queued reads
-  uint64_t queued_bytes = 0;
+  mg::Ring ring;
   uint64_t next_ticket = 1;
-  std::deque<mg::Request*> queue;                           // requests with unscheduled reads
-  std::map<uint64_t, std::unique_ptr<mg::Request>> live;    // every tracked request
+  std::deque<mg::Request*> queue;                          // requests with unscheduled reads
+  std::map<uint64_t, std::unique_ptr<mg::Request>> live;   // every tracked request
   mg::Slot slot[2];
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
@@ -103,12 +91,6 @@ static int slot_alloc(Slot& s, uint64_t reads, uint64_t bases, uint64_t cands) {
       return set_error(MG_ERR_OOM, "pinned step buffers");
     s.cap_reads = reads;
   }
-  if (bases > s.cap_bases) {
-    if (s.h_bases) cudaFreeHost(s.h_bases);
-    s.h_bases = nullptr;
-    if (cudaMallocHost((void**)&s.h_bases, bases) != cudaSuccess) return set_error(MG_ERR_OOM, "pinned step buffers");
-    s.cap_bases = bases;
-  }
   if (cands > s.cap_cands) {
     if (s.h_cands) cudaFreeHost(s.h_cands);
     s.h_cands = nullptr;
@@ -117,100 +99,114 @@ static int slot_alloc(Slot& s, uint64_t reads, uint64_t bases, uint64_t cands) {
     s.cap_cands = cands;
   }
   if (ensure_workspace(s.ws, reads, bases, true)) return MG_ERR_OOM;
-  if (s.ws.cands.alloc(std::max<uint64_t>(cands, 1) * sizeof(mg_candidate))) return set_error(MG_ERR_OOM, "step candidates");
+  if (s.ws.cands.alloc(std::max<uint64_t>(s.cap_cands, 1) * sizeof(mg_candidate)))
+    return set_error(MG_ERR_OOM, "step candidates");
   return MG_OK;
 }
 
 static void slot_free(Slot& s) {
   if (s.st) cudaStreamDestroy(s.st);
   if (s.h_offs) cudaFreeHost(s.h_offs);
-  if (s.h_bases) cudaFreeHost(s.h_bases);
   if (s.h_reads) cudaFreeHost(s.h_reads);
   if (s.h_cands) cudaFreeHost(s.h_cands);
   s.ws.release();
 }
 
 // Form a step from the queue (server lock held) and launch it on the slot's stream.
-static bool form_step(mg_server* sv, Slot& s) {
+static void form_step(mg_server* sv, Slot& s) {
   s.parts.clear();
   s.n = 0;
   uint64_t nb = 0;
-  while (!sv->queue.empty() && s.n < sv->step_reads) {
+  while (!sv->queue.empty() && s.n < sv->step_reads && nb < sv->step_bases) {
     Request* r = sv->queue.front();
-    uint64_t take = std::min(r->n - r->next, sv->step_reads - s.n);
-    // respect the base budget, but always take at least one read
-    uint64_t got = 0, b = 0;
-    while (got < take) {
-      uint64_t L = r->offs[r->next + got + 1] - r->offs[r->next + got];
-      if (nb + b + L > sv->step_bases && (s.n + got) > 0) break;
-      b += L;
-      got++;
+    const uint64_t take = std::min(r->n - r->next, sv->step_reads - s.n);
+    uint64_t got = take;
+    // respect the base budget, but a step always carries at least one read
+    const uint64_t room = sv->step_bases - nb;
+    if (r->offs[r->next + got] - r->offs[r->next] > room) {
+      uint64_t lo = 0, hi = take;  // largest got with bytes <= room
+      while (lo < hi) {
+        uint64_t mid = (lo + hi + 1) / 2;
+        if (r->offs[r->next + mid] - r->offs[r->next] <= room) lo = mid;
+        else hi = mid - 1;
+      }
+      got = std::max<uint64_t>(lo, s.n == 0 ? 1 : 0);
     }
     if (got == 0) break;
     s.parts.push_back(Part{r, r->next, got});
+    nb += r->offs[r->next + got] - r->offs[r->next];
     r->next += got;
     s.n += got;
-    nb += b;
     if (r->next == r->n) sv->queue.pop_front();
-    if (nb >= sv->step_bases) break;
   }
-  if (s.n == 0) return false;
+  s.busy = true;
+  s.launch_rc = MG_OK;
+  if (s.n == 0) return;
   if (slot_alloc(s, s.n, std::max<uint64_t>(nb, sv->step_bases), std::max<uint64_t>(s.cap_cands, 16 * s.n + 1024))) {
     s.launch_rc = MG_ERR_OOM;
-    s.busy = true;
-    return true;
+    return;
   }
-  // pack the reads (offsets rebased) into the pinned staging buffers
+  // offsets rebased into the step; bases copied segment by segment from the ring
   uint64_t at = 0, ob = 0;
   s.h_offs[0] = 0;
+  cudaError_t e = cudaSuccess;
   for (const Part& p : s.parts) {
     const uint64_t b0 = p.req->offs[p.first], b1 = p.req->offs[p.first + p.count];
-    std::memcpy(s.h_bases + ob, p.req->bases.data() + b0, b1 - b0);
     for (uint64_t i = 0; i < p.count; i++) s.h_offs[at + i + 1] = ob + (p.req->offs[p.first + i + 1] - b0);
+    if (e == cudaSuccess && b1 > b0)
+      e = cudaMemcpyAsync(s.ws.bases.as<uint8_t>() + ob, p.req->bases + b0, b1 - b0, cudaMemcpyHostToDevice, s.st);
     at += p.count;
     ob += b1 - b0;
   }
-  mg_index* ix = sv->ix;
-  s.launch_rc = MG_OK;
-  cudaError_t e = cudaMemcpyAsync(s.ws.offs.p, s.h_offs, (s.n + 1) * 8, cudaMemcpyHostToDevice, s.st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(s.ws.bases.p, s.h_bases, ob, cudaMemcpyHostToDevice, s.st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s.ws.offs.p, s.h_offs, (s.n + 1) * 8, cudaMemcpyHostToDevice, s.st);
   if (e != cudaSuccess) {
     s.launch_rc = set_error(MG_ERR_CUDA, cudaGetErrorString(e));
-  } else {
-    s.launch_rc = run_pipeline(ix, s.ws, s.n, s.ws.offs.as<uint64_t>(), s.ws.bases.as<uint8_t>(),
-                               s.ws.reads.as<mg_read_result>(), s.ws.cands.as<mg_candidate>(), s.cap_cands, s.st, false);
-    if (s.launch_rc == MG_OK &&
-        cudaMemcpyAsync(s.h_reads, s.ws.reads.p, s.n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, s.st) !=
-            cudaSuccess)
-      s.launch_rc = MG_ERR_CUDA;
+    return;
   }
-  s.busy = true;
-  return true;
+  s.launch_rc = run_pipeline(sv->ix, s.ws, s.n, s.ws.offs.as<uint64_t>(), s.ws.bases.as<uint8_t>(),
+                             s.ws.reads.as<mg_read_result>(), s.ws.cands.as<mg_candidate>(), s.cap_cands, s.st, false);
+  if (s.launch_rc == MG_OK &&
+      cudaMemcpyAsync(s.h_reads, s.ws.reads.p, s.n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, s.st) != cudaSuccess)
+    s.launch_rc = MG_ERR_CUDA;
 }
 
 // Wait for a launched step and hand its results to the requests (server lock not held while
-// waiting).
+// waiting on the device).
 static void drain_step(mg_server* sv, Slot& s) {
   int rc = s.launch_rc;
-  uint64_t total = 0;
-  if (rc == MG_OK) rc = finish_errors(s.ws, s.st, &total);
-  if (rc == MG_ERR_OOM && total > s.cap_cands) {
-    // the step produced more candidates than its buffer holds: rerun it with room for all
-    if (slot_alloc(s, s.n, s.cap_bases, total + 1024) == MG_OK) {
-      rc = run_pipeline(sv->ix, s.ws, s.n, s.ws.offs.as<uint64_t>(), s.ws.bases.as<uint8_t>(),
+  Counters c;
+  if (rc != MG_OK) cudaStreamSynchronize(s.st);  // copies from the ring may still be in flight
+  auto run = [&]() {
+    return run_pipeline(sv->ix, s.ws, s.n, s.ws.offs.as<uint64_t>(), s.ws.bases.as<uint8_t>(),
                         s.ws.reads.as<mg_read_result>(), s.ws.cands.as<mg_candidate>(), s.cap_cands, s.st, false);
-      if (rc == MG_OK &&
-          cudaMemcpyAsync(s.h_reads, s.ws.reads.p, s.n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, s.st) !=
-              cudaSuccess)
-        rc = MG_ERR_CUDA;
-      if (rc == MG_OK) rc = finish_errors(s.ws, s.st, &total);
-    }
+  };
+  auto complete = [&]() {
+    return complete_pipeline(sv->ix, s.ws, s.n, s.ws.offs.as<uint64_t>(), s.ws.bases.as<uint8_t>(),
+                             s.ws.reads.as<mg_read_result>(), s.ws.cands.as<mg_candidate>(), s.cap_cands, s.st,
+                             false, &c);
+  };
+  bool reran = false;
+  if (rc == MG_OK && s.n) {
+    rc = complete();
+    reran = c.reran;
   }
-  if (rc == MG_OK && total) {
-    if (cudaMemcpyAsync(s.h_cands, s.ws.cands.p, total * sizeof(mg_candidate), cudaMemcpyDeviceToHost, s.st) !=
-            cudaSuccess ||
+  if (rc == MG_OK && (c.err & kErrOutput) && c.n_cands > s.cap_cands) {
+    // more candidates than the step buffer holds: rerun the step with room for all of them
+    rc = slot_alloc(s, s.n, s.ws.bases.n, c.n_cands + 1024);
+    if (rc == MG_OK) rc = run();
+    if (rc == MG_OK) rc = complete();
+    reran = true;
+  }
+  // a rejected read fails its own request only (below); any other error fails the step
+  const int step_bits = c.err & ~(kErrBadInput | kErrLimit);
+  if (rc == MG_OK && step_bits) rc = error_status(step_bits);
+  if (rc == MG_OK && s.n) {
+    if ((reran && cudaMemcpyAsync(s.h_reads, s.ws.reads.p, s.n * sizeof(mg_read_result), cudaMemcpyDeviceToHost,
+                                  s.st) != cudaSuccess) ||
+        (c.n_cands && cudaMemcpyAsync(s.h_cands, s.ws.cands.p, c.n_cands * sizeof(mg_candidate),
+                                      cudaMemcpyDeviceToHost, s.st) != cudaSuccess) ||
         cudaStreamSynchronize(s.st) != cudaSuccess)
-      rc = MG_ERR_CUDA;
+      rc = set_error(MG_ERR_CUDA, "step results");
   }
   std::lock_guard<std::mutex> lk(sv->mu);
   uint64_t at = 0;
@@ -221,6 +217,10 @@ static void drain_step(mg_server* sv, Slot& s) {
     } else {
       for (uint64_t i = 0; i < p.count; i++) {
         mg_read_result rr = s.h_reads[at + i];
+        if (rr.strand == MG_READ_BAD_BYTE || rr.strand == MG_READ_TOO_LARGE) {
+          if (!r->error) r->error = rr.strand == MG_READ_BAD_BYTE ? MG_ERR_BADINPUT : MG_ERR_LIMIT;
+          continue;
+        }
         const uint32_t nc = rr.n_fwd + rr.n_rc;
         const uint64_t dst = r->cands.size();
         r->cands.insert(r->cands.end(), s.h_cands + rr.cand_off, s.h_cands + rr.cand_off + nc);
@@ -232,7 +232,10 @@ static void drain_step(mg_server* sv, Slot& s) {
     at += p.count;
     if (r->done == r->n) {
       r->complete = true;
-      sv->queued_bytes -= r->bases.size() + r->offs.size() * 8;
+      if (!r->released) {
+        sv->ring.release(r->ring_at);
+        r->released = true;
+      }
     }
   }
   s.parts.clear();
@@ -247,7 +250,7 @@ static void server_loop(mg_server* sv) {
   for (;;) {
     sv->cv_work.wait(lk, [&] { return sv->stop || !sv->queue.empty() || sv->slot[0].busy || sv->slot[1].busy; });
     if (sv->stop && !sv->slot[0].busy && !sv->slot[1].busy) break;
-    // launch into every free slot while there is work (the launch is asynchronous)
+    // launch into every free slot while there is work (asynchronous)
     for (int i = 0; i < 2; i++) {
       Slot& s = sv->slot[(oldest + i) % 2];
       if (!s.busy && !sv->queue.empty()) form_step(sv, s);
@@ -282,19 +285,25 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
   mg_server_config c = cfg ? *cfg : mg_server_config{0, 0, 0};
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  uint64_t budget = c.device_budget ? c.device_budget : (uint64_t)(free_b / 4);
-  // per read of a step: ~300 bases, the result, 4 staging + 16 output candidates, overflow lists
+  // device memory for the two step slots: ~0.6 KB per read of a step
   const uint64_t per_read = 320 + 16 + 20 * sizeof(mg_candidate) + 16;
+  const uint64_t dev_budget = c.device_budget ? c.device_budget : (uint64_t)(free_b / 4);
   uint64_t reads = c.max_inflight_reads ? c.max_inflight_reads : 262144;
-  reads = std::max<uint64_t>(1024, std::min<uint64_t>(reads, budget / 2 / per_read));
+  reads = std::max<uint64_t>(1024, std::min<uint64_t>(reads, dev_budget / 2 / per_read));
   sv->step_reads = reads;
   sv->step_bases = reads * 320;
   sv->max_requests = c.max_requests ? c.max_requests : 4096;
-  sv->queue_budget = std::max<uint64_t>(budget, 64ull << 20);
+  // pinned ring for queued requests: 4 steps' worth of reads, at least 64 MB
+  sv->ring.cap = std::max<uint64_t>(64ull << 20, 4 * (sv->step_bases + (sv->step_reads + 1) * 8));
+  if (cudaMallocHost((void**)&sv->ring.base, sv->ring.cap) != cudaSuccess) {
+    delete sv;
+    return set_error(MG_ERR_OOM, "pinned request ring");
+  }
   for (auto& s : sv->slot) {
     if (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess ||
         slot_alloc(s, sv->step_reads, sv->step_bases, 16 * sv->step_reads + 1024) != MG_OK) {
       for (auto& t : sv->slot) slot_free(t);
+      cudaFreeHost(sv->ring.base);
       delete sv;
       return set_error(MG_ERR_OOM, "server step buffers");
     }
@@ -309,35 +318,36 @@ int mg_server_submit(mg_server* sv, const mg_batch* b, uint64_t* ticket) {
   const uint64_t n = b->n_reads;
   const uint64_t nb = n ? b->offsets[n] : 0;
   if (n && b->offsets[0] != 0) return set_error(MG_ERR_INVAL, "offsets[0] must be 0");
-  for (uint64_t i = 0; i < nb; i++)
-    if (!has_complement(b->bases[i])) return set_error(MG_ERR_BADINPUT, "a read holds a byte without a reverse complement");
   for (uint64_t i = 0; i < n; i++)
     if (b->offsets[i + 1] < b->offsets[i] || b->offsets[i + 1] - b->offsets[i] > 65535)
       return set_error(MG_ERR_LIMIT, "read longer than 65535 bases");
-  const uint64_t bytes = nb + (n + 1) * 8;
+  const uint64_t len = nb + (n + 1) * 8 + 16;
   std::unique_ptr<Request> r(new Request());
+  r->n = n;
   {
     std::lock_guard<std::mutex> lk(sv->mu);
-    if (sv->live.size() >= sv->max_requests || (sv->queued_bytes > 0 && sv->queued_bytes + bytes > sv->queue_budget))
+    if (len > sv->ring.cap) return set_error(MG_ERR_LIMIT, "request larger than the server's request memory");
+    if (sv->live.size() >= sv->max_requests || !sv->ring.alloc(len, &r->ring_at))
       return set_error(MG_ERR_BUSY, "server at capacity");
-    sv->queued_bytes += bytes;  // reserved before the copy
+    r->offs = (uint64_t*)(sv->ring.base + r->ring_at);
+    r->bases = sv->ring.base + r->ring_at + (n + 1) * 8;
   }
-  r->n = n;
+  std::memcpy(r->offs, b->offsets, (n + 1) * 8);
+  std::memcpy(r->bases, b->bases, nb);
   try {
-    r->offs.assign(b->offsets, b->offsets + n + 1);
-    r->bases.assign(b->bases, b->bases + nb);
     r->reads.resize(n);
   } catch (...) {
     std::lock_guard<std::mutex> lk(sv->mu);
-    sv->queued_bytes -= bytes;
-    return set_error(MG_ERR_OOM, "host memory for the request copy");
+    sv->ring.release(r->ring_at);
+    return set_error(MG_ERR_OOM, "host memory for the results");
   }
   std::lock_guard<std::mutex> lk(sv->mu);
   r->ticket = sv->next_ticket++;
   *ticket = r->ticket;
   if (n == 0) {
     r->complete = true;
-    sv->queued_bytes -= bytes;
+    r->released = true;
+    sv->ring.release(r->ring_at);
   } else {
     sv->queue.push_back(r.get());
   }
@@ -351,7 +361,7 @@ static int take_result(mg_server* sv, std::map<uint64_t, std::unique_ptr<Request
   if (r->error) {
     int e = r->error;
     sv->live.erase(it);
-    return set_error(e, "request failed on the device");
+    return set_error(e, mg_strerror(e));
   }
   out->n_cands = r->cands.size();
   if (r->cands.size() > out->cand_cap) return set_error(MG_ERR_OOM, "candidate output buffer too small");
@@ -392,6 +402,7 @@ void mg_server_destroy(mg_server* sv) {
   if (sv->th.joinable()) sv->th.join();
   cudaSetDevice(sv->ix->device);
   for (auto& s : sv->slot) slot_free(s);
+  if (sv->ring.base) cudaFreeHost(sv->ring.base);
   delete sv;
 }
 

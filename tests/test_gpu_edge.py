@@ -107,3 +107,27 @@ def test_long_reads_go_through_every_tier(golden):
     ref = g.refs.seq(int(np.argmax(g.refs.lengths()))).tobytes()
     seqs = [ref[0:20000], ref[5:25005], ref[100:60100]]
     check_against_oracle(gix, oix, seqs)
+
+
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_many_candidates_grow_staging_arena(tmp_path, form):
+    """Every read matches 24 identical references: 5,000 reads need 120,000 staging entries,
+    more than a fresh workspace holds, so the batch runs again with a larger staging arena and
+    still equals the oracle."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(17)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 20000)]
+    refs = [core] * 24 + [acgt[rng.integers(0, 4, 20000)] for _ in range(4)]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))])
+    path = tmp_path / "dup.mhm"
+    image.tofile(path)
+    gix = M.Index(image)
+    oix = O.Index(str(path))
+    starts = rng.integers(0, 20000 - 150, 5000)
+    seqs = [core[s:s + 150].tobytes() for s in starts]
+    r = check_against_oracle(gix, oix, seqs, form)
+    assert (r.reads["n_fwd"] + r.reads["n_rc"]).sum() >= 24 * 5000

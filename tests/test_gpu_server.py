@@ -90,17 +90,23 @@ def test_admission_and_errors(golden):
     assert sv.submit(d, o) is None
     sv.wait(t1)
     sv.wait(t2)
-    assert sv.submit(d, o) is not None
+    t3 = sv.submit(d, o)
+    assert t3 is not None
+    same(sv.wait(t3), ix.classify(d, o))
     # unknown ticket
     with pytest.raises(M.MirageError) as e:
         sv.poll(987654)
     assert e.value.code == -8
-    # a byte without a reverse complement is refused at submit
+    # a byte without a reverse complement fails its own request only, also when the request
+    # shares a step with another (1024-read steps, 3000-read requests)
     bad = d.copy()
-    bad[10] = ord("X")
+    bad[int(o[2500]) + 3] = ord("X")
+    tb = sv.submit(bad, o)
+    tg = sv.submit(d, o)
     with pytest.raises(M.MirageError) as e:
-        sv.submit(bad, o)
+        sv.wait(tb)
     assert e.value.code == -6
+    same(sv.wait(tg), ix.classify(d, o))
     # empty request completes at once
     t = sv.submit(np.zeros(0, np.uint8), np.zeros(1, np.uint64))
     r = sv.wait(t)
