@@ -166,6 +166,23 @@ int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off,
                         const uint64_t* r_off, const uint32_t* runs, float* score, float* pct,
                         float* rel, float* highest);
 
+/* mg_score_candidates for callers that may not allocate device memory (their device memory is
+ * held by another allocator, or a cudaFree's device-wide synchronisation would stall other
+ * work). No counterpart in the reference. Same arguments and outputs, all of them DEVICE
+ * pointers on ix's device, plus a stream (NULL = the index's stream); it calls no cudaMalloc or
+ * cudaFree. Its working memory is a fixed 4,849,920-byte array that the library holds on every
+ * GPU that loads it, until exit; that caps a query strand at 2048 bases (longer ones: MG_ERR_LIMIT,
+ * and their candidates are left unscored). The first call on each device looks up the array's
+ * device address; make that first call before any stream capture. Every call on a device uses the
+ * same array: calls whose GPU work overlapped would race on it, so the library serialises its
+ * calls and each returns after its GPU work has ended. A candidate reference or run outside its
+ * reference or query returns MG_ERR_INVAL. */
+int mg_score_candidates_noalloc(mg_index* ix, uint64_t n_strands, const uint64_t* d_q_off,
+                                const uint8_t* d_bases, const uint64_t* d_c_off,
+                                const uint32_t* d_cand_ref, const uint64_t* d_r_off,
+                                const uint32_t* d_runs, float* d_score, float* d_pct,
+                                float* d_rel, float* d_highest, void* stream);
+
 /* Served form: continuous batching against the HBM-resident index. Requests are admitted
  * into slots while device memory allows, coalesced into the running persistent kernel, and
  * completed independently. */

@@ -27,7 +27,7 @@ EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_insp
            "mg_set_timing", "mg_last_kernel_times", "mg_bucket_sizes",
            "mg_build_image", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
-           "mg_score_candidates", "mg_server_create", "mg_server_submit", "mg_server_poll",
+           "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_poll",
            "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error", "mg_logs_open", "mg_logs_write",
            "mg_logs_close", "mg_make_results_dir", "mg_index_reference"]
 
@@ -81,6 +81,7 @@ def lib() -> C.CDLL:
         L.mg_classify_device.argtypes = [vp, u64, vp, vp, vp, vp, u64, vp, vp]
         L.mg_classify_device_sync.argtypes = [vp, vp, C.POINTER(u64)]
         L.mg_score_candidates.argtypes = [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.mg_score_candidates_noalloc.argtypes = [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.mg_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
         L.mg_server_submit.argtypes = [vp, C.POINTER(_Batch), C.POINTER(u64)]
         L.mg_server_poll.argtypes = [vp, u64, C.POINTER(_Result)]
