@@ -248,95 +248,146 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s: float, fracs=(0.25, 0.5, 0.75, 0.9)):
+def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s: float, clients: int = 4,
+                 fracs=(0.25, 0.5, 0.75, 0.9)):
     """Served form (mg_server_*): saturated throughput, then latency under Poisson arrivals at
     fractions of it. Requests are contiguous slices of the host reads with log-uniform sizes in
-    [1, 50000] reads; each submit copies its request from host memory, each wait returns it."""
+    [1, 50000] reads. `clients` threads submit and wait through the C ABI, each with its own
+    preallocated result buffers; every submit copies its request from host memory and every wait
+    copies its results out, inside the measurement."""
     import collections
+    import ctypes as C
 
-    rng = np.random.default_rng(seed)
     n = len(offs) - 1
     max_req = min(50000, n)
+    L = M.lib()
+    mean_size = (max_req - 1) / np.log(max_req) if max_req > 1 else 1.0
 
-    def draw():
-        size = int(np.exp(rng.uniform(0.0, np.log(max_req + 1))))
-        size = max(1, min(size, max_req))
-        st = int(rng.integers(0, n - size + 1))
-        return st, size
+    class Client:
+        def __init__(self, k):
+            self.rng = np.random.default_rng(seed + 1000 * k)
+            self.reads = np.empty(max_req, dtype=M.READ_DTYPE)
+            self.cap = 64 * max_req
+            self.cands = np.empty(self.cap, dtype=M.CAND_DTYPE)
+            self.res = M._Result(self.reads.ctypes.data, self.cands.ctypes.data, self.cap, 0)
 
-    def request(st, size):
-        o = offs[st:st + size + 1]
-        return bases[int(o[0]):int(o[-1])], o - o[0]
+        def request(self):
+            size = int(np.exp(self.rng.uniform(0.0, np.log(max_req + 1))))
+            size = max(1, min(size, max_req))
+            st = int(self.rng.integers(0, n - size + 1))
+            o = offs[st:st + size + 1]
+            ob = np.ascontiguousarray(o - o[0])
+            b = bases[int(o[0]):int(o[-1])]
+            return size, M._Batch(size, ob.ctypes.data, b.ctypes.data), (ob, b)
+
+        def submit(self, req):
+            t = C.c_uint64()
+            while True:
+                rc = L.mg_server_submit(sv.h, C.byref(req[1]), C.byref(t))
+                if rc != -9:
+                    break
+                time.sleep(5e-5)  # admission refused: retry (the wait counts toward latency)
+            if rc != 0:
+                raise RuntimeError(f"mg_server_submit: {rc}")
+            return t.value
+
+        def wait(self, ticket):
+            self.res.n_cands = 0
+            rc = L.mg_server_wait(sv.h, ticket, C.byref(self.res), 600000)
+            if rc != 1:
+                raise RuntimeError(f"mg_server_wait: {rc} {L.mg_last_error()}")
 
     sv = M.Server(ix)
+    cl = [Client(k) for k in range(clients)]
     try:
-        for _ in range(8):  # warm-up
-            sv.wait(sv.submit(*request(*draw())))
-        # saturated: keep the server full for ~level_s seconds
-        q, total, t0 = collections.deque(), 0, time.perf_counter()
-        while time.perf_counter() - t0 < level_s:
-            st, size = draw()
-            b, o = request(st, size)
-            t = sv.submit(b, o)
-            while t is None:
-                sv.wait(q.popleft())
-                t = sv.submit(b, o)
-            q.append(t)
-            total += size
-        while q:
-            sv.wait(q.popleft())
-        sat = total / (time.perf_counter() - t0)
-        mean_size = (max_req - 1) / np.log(max_req) if max_req > 1 else 1.0
+        for c in cl:  # warm-up
+            for _ in range(4):
+                c.wait(c.submit(c.request()))
+
+        # saturated: each client keeps up to 4 requests outstanding for ~level_s seconds
+        totals = [0] * clients
+
+        def closed(k):
+            c, q = cl[k], collections.deque()
+            t_end = time.perf_counter() + level_s
+            while time.perf_counter() < t_end:
+                req = c.request()
+                q.append(c.submit(req))
+                totals[k] += req[0]
+                if len(q) >= 4:
+                    c.wait(q.popleft())
+            while q:
+                c.wait(q.popleft())
+
+        t0 = time.perf_counter()
+        th = [threading.Thread(target=closed, args=(k,)) for k in range(clients)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        sat = sum(totals) / (time.perf_counter() - t0)
+
         levels = []
         for f in fracs:
-            rate = f * sat / mean_size  # requests per second
-            pending = collections.deque()
-            lat, done_reads = [], [0]
-            cv = threading.Condition()
-            finished = [False]
+            rate = f * sat / mean_size / clients  # requests per second per client
+            lat, done = [], [0]
+            lock = threading.Lock()
 
-            def waiter():
-                while True:
+            def open_loop(k):
+                c = cl[k]
+                pending = collections.deque()
+                cv = threading.Condition()
+                fin = [False]
+                mine = []
+
+                def waiter():
+                    while True:
+                        with cv:
+                            while not pending and not fin[0]:
+                                cv.wait()
+                            if not pending:
+                                return
+                            t, arrive, size = pending.popleft()
+                        c.wait(t)
+                        mine.append((time.perf_counter() - arrive, size))
+
+                w = threading.Thread(target=waiter)
+                w.start()
+                t0 = time.perf_counter()
+                arrive = t0
+                while arrive - t0 < level_s:
+                    arrive += c.rng.exponential(1.0 / rate)
+                    now = time.perf_counter()
+                    if arrive > now:
+                        time.sleep(arrive - now)
+                    req = c.request()
+                    t = c.submit(req)
                     with cv:
-                        while not pending and not finished[0]:
-                            cv.wait()
-                        if not pending:
-                            return
-                        t, arrive, size = pending.popleft()
-                    sv.wait(t)
-                    lat.append(time.perf_counter() - arrive)
-                    done_reads[0] += size
-
-            th = threading.Thread(target=waiter)
-            th.start()
-            t0 = time.perf_counter()
-            arrive = t0
-            while arrive - t0 < level_s:
-                arrive += rng.exponential(1.0 / rate)
-                now = time.perf_counter()
-                if arrive > now:
-                    time.sleep(arrive - now)
-                st, size = draw()
-                b, o = request(st, size)
-                t = sv.submit(b, o)
-                while t is None:  # admission refused: the wait counts toward latency
-                    time.sleep(5e-5)
-                    t = sv.submit(b, o)
+                        pending.append((t, arrive, req[0]))
+                        cv.notify()
                 with cv:
-                    pending.append((t, arrive, size))
+                    fin[0] = True
                     cv.notify()
-            with cv:
-                finished[0] = True
-                cv.notify()
-            th.join()
+                w.join()
+                with lock:
+                    lat.extend(x for x, _ in mine)
+                    done[0] += sum(sz for _, sz in mine)
+
+            t0 = time.perf_counter()
+            th = [threading.Thread(target=open_loop, args=(k,)) for k in range(clients)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
             span = time.perf_counter() - t0
             ms = np.array(lat) * 1000
-            levels.append({"offered_frac": f, "offered_reads_s": f * sat, "achieved_reads_s": done_reads[0] / span,
+            levels.append({"offered_frac": f, "offered_reads_s": f * sat, "achieved_reads_s": done[0] / span,
                            "requests": len(lat), "p50_ms": float(np.percentile(ms, 50)),
                            "p99_ms": float(np.percentile(ms, 99))})
         return {"saturated": {"value": sat, "unit": "reads/s"},
                 "requests": "log-uniform 1..%d reads, contiguous slices of the batch" % max_req,
-                "arrivals": "Poisson", "seconds_per_level": level_s, "load": levels}
+                "clients": clients, "arrivals": "Poisson (one process per client thread)",
+                "seconds_per_level": level_s, "load": levels}
     finally:
         sv.close()
 

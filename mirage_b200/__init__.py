@@ -336,8 +336,8 @@ class Server:
         n = self._pending.get(ticket, 0)
         cap = max(1024, 8 * n)
         while True:
-            reads = np.zeros(n, dtype=READ_DTYPE)
-            cands = np.zeros(cap, dtype=CAND_DTYPE)
+            reads = np.empty(n, dtype=READ_DTYPE)
+            cands = np.empty(cap, dtype=CAND_DTYPE)
             r = _Result(reads.ctypes.data, cands.ctypes.data, cap, 0)
             rc = fn(self.h, ticket, C.byref(r), *extra)
             if rc == -3 and r.n_cands > cap:

@@ -214,18 +214,22 @@ static void drain_step(mg_server* sv, Slot& s) {
     Request* r = p.req;
     if (rc != MG_OK) {
       r->error = rc;
-    } else {
+    } else if (!r->error) {
+      // the segment's candidates are contiguous in the step's output (read order): one copy
+      const mg_read_result* src = s.h_reads + at;
+      const mg_read_result& last = src[p.count - 1];
+      const uint64_t c0 = src[0].cand_off, c1 = (uint64_t)last.cand_off + last.n_fwd + last.n_rc;
+      const uint64_t base = r->cands.size();
+      r->cands.insert(r->cands.end(), s.h_cands + c0, s.h_cands + c1);
+      mg_read_result* dst = r->reads.data() + p.first;
       for (uint64_t i = 0; i < p.count; i++) {
-        mg_read_result rr = s.h_reads[at + i];
+        mg_read_result rr = src[i];
         if (rr.strand == MG_READ_BAD_BYTE || rr.strand == MG_READ_TOO_LARGE) {
-          if (!r->error) r->error = rr.strand == MG_READ_BAD_BYTE ? MG_ERR_BADINPUT : MG_ERR_LIMIT;
-          continue;
+          r->error = rr.strand == MG_READ_BAD_BYTE ? MG_ERR_BADINPUT : MG_ERR_LIMIT;
+          break;
         }
-        const uint32_t nc = rr.n_fwd + rr.n_rc;
-        const uint64_t dst = r->cands.size();
-        r->cands.insert(r->cands.end(), s.h_cands + rr.cand_off, s.h_cands + rr.cand_off + nc);
-        rr.cand_off = (uint32_t)dst;
-        r->reads[p.first + i] = rr;
+        rr.cand_off = (uint32_t)(rr.cand_off - c0 + base);
+        dst[i] = rr;
       }
     }
     r->done += p.count;
