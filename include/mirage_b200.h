@@ -117,11 +117,12 @@ int mg_eval_logf(mg_index* ix, const float* x, float* out, uint64_t n);
 
 /* Diagnostics (no counterpart in the reference). mg_set_timing(ix, 1) records CUDA events
  * around every kernel of each following classification call; mg_last_kernel_times writes the
- * last call's device times in milliseconds: [warp tier (or the plain form's kernel), block
- * tier, global-memory tier, output compaction]. mg_bucket_sizes returns the number of
- * postings stored under each of n 28-bit hashes (the index directory, read on the device). */
+ * last call's device times in milliseconds, 5 entries: [dual-strand warp tier (or the plain
+ * form's kernel), lean + general warp tiers, block tier, global-memory tier, output
+ * compaction]. mg_bucket_sizes returns the number of postings stored under each of n 28-bit
+ * hashes (the index directory, read on the device). */
 int mg_set_timing(mg_index* ix, int on);
-int mg_last_kernel_times(mg_index* ix, float* ms4);
+int mg_last_kernel_times(mg_index* ix, float* ms5);
 int mg_bucket_sizes(mg_index* ix, const uint32_t* hashes, uint32_t* counts, uint64_t n);
 
 /* Replaces Hashmap::BuildHashmapTable + SaveHashmapTableV3 (Hashmap.cpp:967, :1701): builds a
@@ -135,8 +136,8 @@ void mg_free(void* p);
 
 /* Plain form. Replaces the reference's per-batch sequence TPrepareGPUAnalysis (Analyser.cpp:
  * 1317) -> CPUGetHighestScore (MatrixCPU.cpp:417) -> strand merge (Analyser.cpp:592-611):
- * one kernel launch per batch, one thread per (read, strand), host buffers in and out with
- * synchronous copies. */
+ * one block per read in one launch per batch (the global-memory tier takes reads beyond its
+ * shared memory), host buffers in and out with synchronous copies. */
 int mg_score_batch(mg_index* ix, const mg_batch* batch, mg_result* out);
 
 /* Batched form: the same results from the fused persistent kernel (warp per read with work

@@ -21,7 +21,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,
           "-Xcompiler", "-ffp-contract=off"]
 
 LIB_SOURCES = ["mg_lib.cu", "mg_server.cu", "mhm.cpp", "mg_output.cu", "mg_noalloc.cu"]
-HEADERS = ["mg_device.cuh", "mg_kernels.cuh", "mg_lean.cuh", "mhm.h", "mg_internal.h", "mg_ring.h"]
+HEADERS = ["mg_device.cuh", "mg_kernels.cuh", "mg_lean.cuh", "mg_dual.cuh", "mhm.h", "mg_internal.h", "mg_ring.h"]
 TOOL_SOURCES = ["mirage_gpu.cpp"]
 
 

@@ -37,12 +37,12 @@ struct DevBuf {
 
 // Device buffers of one classification call in flight (a call owns one at a time).
 struct Workspace {
-  DevBuf offs, bases, reads, stage, arena, cands, ctr, ovf, sums, gws;
+  DevBuf offs, bases, reads, stage, arena, cands, ctr, ovf, sums, gws, chain;
   void release() {
-    for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws}) b->release();
+    for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws, &chain}) b->release();
   }
   size_t bytes() const {
-    return offs.n + bases.n + reads.n + stage.n + arena.n + cands.n + ctr.n + ovf.n + sums.n + gws.n;
+    return offs.n + bases.n + reads.n + stage.n + arena.n + cands.n + ctr.n + ovf.n + sums.n + gws.n + chain.n;
   }
 };
 
@@ -50,8 +50,12 @@ int set_error(int code, const std::string& msg);
 // Size ws for n_reads reads (n_bases bases when host_io: the input and result buffers too).
 int ensure_workspace(Workspace& ws, uint64_t n_reads, uint64_t n_bases, bool host_io);
 // Queue the fused pipeline (warp, block and global tiers, then compaction) on stream st.
+// chain (optional, device, 16 bytes): for one chunk of a larger batch, [0] the candidates of the
+// earlier chunks (output offsets continue from there and the count is advanced), [8] the batch's
+// error bits (accumulated instead of the per-call counter).
 int run_pipeline(mg_index* ix, Workspace& ws, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
-                 mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain);
+                 mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain,
+                 unsigned long long* chain = nullptr);
 // Wait for st, read the error word and the candidate count of the call that used ws.
 int finish_errors(Workspace& ws, cudaStream_t st, uint64_t* n_cands);
 // The pipeline's counters after the stream drains.
@@ -79,13 +83,18 @@ struct mg_index {
   mg::DevBuf dir, post, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals;
   mg::Workspace ws;   // workspace of the synchronous entry points
   cudaStream_t stream = nullptr;
+  // chunked batched form: copy streams and per-chunk events (made on first use)
+  static constexpr int kMaxChunks = 8;
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in[kMaxChunks], ev_done[kMaxChunks];
+  bool chunk_made = false;
   std::mutex mu;
   mg_index_info info{};
   uint64_t device_bytes = 0;
   // optional per-kernel timing of the last pipeline (events on the launching stream)
   bool timing = false;
   bool events_made = false;
-  cudaEvent_t ev[5];
+  cudaEvent_t ev[6];
   // arguments of the last mg_classify_device launch, for its completion in the sync call
   struct {
     uint64_t n = 0, cap = 0;

@@ -321,20 +321,25 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
 }
 
 // Strand merge (Analyser.cpp:592-611), the log skip rule (:388) and the staging write of one
-// read's scored candidates (forward strand first). Called by one thread.
-__device__ __forceinline__ void write_read_result(const BatchDev& b, uint32_t r, bool bad, const uint32_t* n,
-                                                  const float* h, mg_candidate* const* cb, mg_candidate* stage,
-                                                  mg_candidate* arena, uint64_t arena_cap,
-                                                  unsigned long long* arena_n, int* errw, int err) {
+// read's scored candidates (forward strand first). Called by one thread; per-strand values are
+// scalars (n0/h0/cb0 forward, n1/h1/cb1 reverse complement).
+__device__ __forceinline__ void write_read_result_s(const BatchDev& b, uint32_t r, bool bad, uint32_t n0,
+                                                    uint32_t n1, float h0, float h1, const mg_candidate* cb0,
+                                                    const mg_candidate* cb1, mg_candidate* stage,
+                                                    mg_candidate* arena, uint64_t arena_cap,
+                                                    unsigned long long* arena_n, int* errw, int err) {
   mg_read_result rr;
   if (bad) {
     err |= kErrBadInput;
     rr = mg_read_result{-1.0f, 0, 0, 0, MG_READ_BAD_BYTE, 0, 0};
   } else {
-    const int ch = h[0] < h[1] ? 1 : 0;  // Analyser.cpp:601
+    const int ch = h0 < h1 ? 1 : 0;  // Analyser.cpp:601
+    const uint32_t nch = ch ? n1 : n0;
+    const float hch = ch ? h1 : h0;
+    const mg_candidate* cbc = ch ? cb1 : cb0;
     uint32_t top = 0;
-    for (uint32_t c = 0; c < n[ch]; c++) top += cb[ch][c].rel == h[ch];
-    const uint32_t tot = n[0] + n[1];
+    for (uint32_t c = 0; c < nch; c++) top += cbc[c].rel == hch;
+    const uint32_t tot = n0 + n1;
     uint32_t where = 0;
     mg_candidate* dst = stage + (uint64_t)r * kSlots;
     if (tot > (uint32_t)kSlots) {
@@ -348,14 +353,21 @@ __device__ __forceinline__ void write_read_result(const BatchDev& b, uint32_t r,
       }
     }
     if (dst) {
-      for (uint32_t c = 0; c < n[0]; c++) dst[c] = cb[0][c];
-      for (uint32_t c = 0; c < n[1]; c++) dst[n[0] + c] = cb[1][c];
+      for (uint32_t c = 0; c < n0; c++) dst[c] = cb0[c];
+      for (uint32_t c = 0; c < n1; c++) dst[n0 + c] = cb1[c];
     }
-    const uint8_t reported = (n[ch] > 0 && h[ch] != 0.0f) ? 1 : 0;  // Analyser.cpp:388
-    rr = mg_read_result{h[ch], where, (uint16_t)n[0], (uint16_t)n[1], (uint8_t)ch, reported, (uint16_t)top};
+    const uint8_t reported = (nch > 0 && hch != 0.0f) ? 1 : 0;  // Analyser.cpp:388
+    rr = mg_read_result{hch, where, (uint16_t)n0, (uint16_t)n1, (uint8_t)ch, reported, (uint16_t)top};
   }
   b.reads[r] = rr;
   if (err) atomicOr(errw, err);
+}
+
+__device__ __forceinline__ void write_read_result(const BatchDev& b, uint32_t r, bool bad, const uint32_t* n,
+                                                  const float* h, mg_candidate* const* cb, mg_candidate* stage,
+                                                  mg_candidate* arena, uint64_t arena_cap,
+                                                  unsigned long long* arena_n, int* errw, int err) {
+  write_read_result_s(b, r, bad, n[0], n[1], h[0], h[1], cb[0], cb[1], stage, arena, arena_cap, arena_n, errw, err);
 }
 
 // Both strands of read r, the strand merge and the staging write. Returns false when the

@@ -18,6 +18,7 @@
 #include "mg_device.cuh"
 #include "mg_kernels.cuh"
 #include "mg_lean.cuh"
+#include "mg_dual.cuh"
 #include "mhm.h"
 
 namespace mg {
@@ -109,8 +110,33 @@ struct StageDev {
   unsigned long long* arena_n;
 };
 
-// Lean warp tier: every read of the batch, one warp per read, work stealing in chunks; reads
-// that do not fit the lean path go to the general warp tier.
+// Dual-strand warp tier: every read of the batch, one warp per read (a half-warp per strand),
+// work stealing in chunks; reads that do not fit go to the lean warp tier.
+__global__ void __launch_bounds__(kW1Warps * 32) k_classify_dual(DevIndex ix, BatchDev b, StageDev sd) {
+  __shared__ DualSmem sm[kW1Warps];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  DualSmem& S = sm[w];
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((uint64_t)base >= b.n) break;
+    const uint64_t end64 = (uint64_t)base + kW1Chunk;
+    const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
+    for (uint32_t r = base; r < end; r++) {
+      if (!process_read_dual(ix, b, r, S, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+        if (lane == 0) {
+          unsigned at = atomicAdd(b.n_ovfL, 1u);
+          b.ovfL[at] = r;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Lean warp tier over the dual tier's leftovers, one warp per read (one strand after the
+// other on all 32 lanes); reads that do not fit the lean path go to the general warp tier.
 struct LeanSmem {
   uint32_t a[8][kLeanE];
   mg_candidate cb[2][kW1C];
@@ -131,22 +157,20 @@ __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp(DevIndex ix, Ba
   lw.z = S.a[6];
   lw.segmax = S.a[7];
   mg_candidate* const cbs[2] = {S.cb[0], S.cb[1]};
+  const uint32_t n = *b.n_ovfL;
   for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if ((uint64_t)base >= b.n) break;
-    const uint64_t end64 = (uint64_t)base + kW1Chunk;
-    const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
-    for (uint32_t r = base; r < end; r++) {
-      if (!process_read_lean(ix, b, r, S.q, lw, cbs, kW1C, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
-        if (lane == 0) {
-          unsigned at = atomicAdd(b.n_ovf0, 1u);
-          b.ovf0[at] = r;
-        }
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(b.workL, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= n) break;
+    const uint32_t r = b.ovfL[item];
+    if (!process_read_lean(ix, b, r, S.q, lw, cbs, kW1C, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+      if (lane == 0) {
+        unsigned at = atomicAdd(b.n_ovf0, 1u);
+        b.ovf0[at] = r;
       }
-      __syncwarp();
     }
+    __syncwarp();
   }
 }
 
@@ -236,15 +260,37 @@ __global__ void k_count_sums(const mg_read_result* reads, uint64_t n, unsigned l
   }
 }
 
-__global__ void k_scan_sums(unsigned long long* block_sums, uint64_t nb, unsigned long long* total) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    unsigned long long run = 0;
-    for (uint64_t i = 0; i < nb; i++) {
-      unsigned long long v = block_sums[i];
-      block_sums[i] = run;
-      run += v;
+// Exclusive scan of the per-block candidate counts, one block of kScanBlock threads in tiles.
+// chain (optional): candidates of earlier chunks of the same batch; the scan starts there and
+// leaves the new running total behind, so chunk offsets are offsets into the batch's output.
+__global__ void __launch_bounds__(kScanBlock) k_scan_sums(unsigned long long* block_sums, uint64_t nb,
+                                                          unsigned long long* total, unsigned long long* chain) {
+  __shared__ unsigned long long s[kScanBlock / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned long long base = chain ? *chain : 0ull;
+  unsigned long long carry = base;
+  for (uint64_t t0 = 0; t0 < nb; t0 += kScanBlock) {
+    const uint64_t i = t0 + threadIdx.x;
+    const unsigned long long v = i < nb ? block_sums[i] : 0ull;
+    unsigned long long x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    *total = run;
+    if (lane == 31) s[wid] = x;
+    __syncthreads();
+    unsigned long long wb = 0, tile = 0;
+    for (int w = 0; w < kScanBlock / 32; w++) {
+      wb += w < wid ? s[w] : 0ull;
+      tile += s[w];
+    }
+    if (i < nb) block_sums[i] = carry + wb + x - v;
+    carry += tile;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *total = carry - base;
+    if (chain) *chain = carry;
   }
 }
 
@@ -501,7 +547,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
   }
   if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
       w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
-      w.ovf.alloc(3 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+      w.ovf.alloc(4 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
@@ -509,10 +555,10 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 }
 
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
-// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1
+// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovfL | 60 workL
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
-                        bool plain) {
+                        bool plain, unsigned long long* chain) {
   uint8_t* ctr = w.ctr.as<uint8_t>();
   CU(cudaMemsetAsync(ctr, 0, 256, st));
   BatchDev b;
@@ -523,7 +569,7 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   b.cands = d_out;
   b.cand_cap = cap;
   b.n_cands = (unsigned long long*)(ctr + 0);
-  b.err = (int*)(ctr + 16);
+  b.err = chain ? (int*)(chain + 1) : (int*)(ctr + 16);
   b.work = (unsigned*)(ctr + 20);
   b.n_ovf1 = (unsigned*)(ctr + 24);
   b.work2 = (unsigned*)(ctr + 28);
@@ -531,6 +577,9 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   b.work3 = (unsigned*)(ctr + 36);
   b.n_ovf0 = (unsigned*)(ctr + 48);
   b.work1 = (unsigned*)(ctr + 52);
+  b.n_ovfL = (unsigned*)(ctr + 56);
+  b.workL = (unsigned*)(ctr + 60);
+  b.ovfL = w.ovf.as<uint32_t>() + 3 * (n + 4);
   b.ovf0 = w.ovf.as<uint32_t>();
   b.ovf1 = w.ovf.as<uint32_t>() + n + 4;
   b.ovf2 = w.ovf.as<uint32_t>() + 2 * (n + 4);
@@ -558,7 +607,12 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
           ix->dix, b, sd, nullptr, nullptr, nullptr, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
       if (tm) CU(cudaEventRecord(ix->ev[2], st));
+      if (tm) CU(cudaEventRecord(ix->ev[3], st));
     } else {
+      int per_smd = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smd, k_classify_dual, kW1Warps * 32, 0);
+      k_classify_dual<<<(unsigned)std::max(1, per_smd) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      if (tm) CU(cudaEventRecord(ix->ev[1], st));
       int per_sm = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_classify_warp, kW1Warps * 32, 0);
       unsigned grid = (unsigned)std::max(1, per_sm) * sms;
@@ -566,22 +620,22 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       int per_sm2 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
       k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
-      if (tm) CU(cudaEventRecord(ix->ev[1], st));
+      if (tm) CU(cudaEventRecord(ix->ev[2], st));
       k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, st>>>(
           ix->dix, b, sd, b.ovf1, b.n_ovf1, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
-      if (tm) CU(cudaEventRecord(ix->ev[2], st));
+      if (tm) CU(cudaEventRecord(ix->ev[3], st));
     }
     CU(cudaGetLastError());
     k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, st>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3,
                                                                    nullptr, nullptr, w.gws.as<uint8_t>(), l3, c3, 1);
-    if (tm) CU(cudaEventRecord(ix->ev[3], st));
+    if (tm) CU(cudaEventRecord(ix->ev[4], st));
     CU(cudaGetLastError());
     const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
     unsigned long long* sums = w.sums.as<unsigned long long>();
     k_count_sums<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums);
-    k_scan_sums<<<1, 32, 0, st>>>(sums, nb, (unsigned long long*)(ctr + 40));
+    k_scan_sums<<<1, kScanBlock, 0, st>>>(sums, nb, (unsigned long long*)(ctr + 40), chain);
     k_scatter<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums, sd, d_out, cap, b.err);
-    if (tm) CU(cudaEventRecord(ix->ev[4], st));
+    if (tm) CU(cudaEventRecord(ix->ev[5], st));
     CU(cudaGetLastError());
   }
   return MG_OK;
@@ -628,6 +682,69 @@ int error_status(int err) {
   return MG_OK;
 }
 
+// Reads per chunk of the batched form with host buffers; a batch of fewer than twice this runs
+// in one piece.
+constexpr uint64_t kChunkReads = 131072;
+constexpr int kRunWhole = 1;
+
+// Batched form with host buffers, in chunks: chunk i's bases are copied on the index's h2d stream
+// while chunk i-1 is classified on its compute stream, and chunk i's read results go back on the
+// d2h stream while chunk i+1 is classified. The chunks share the device output: the compaction
+// continues the candidate offsets of the earlier chunks (run_pipeline's chain), so cand_off is an
+// offset into the whole batch's candidates, as in one piece. Returns kRunWhole when a chunk's
+// staging arena overflowed (the caller then runs the batch in one piece, which grows it).
+static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, mg_result* out) {
+  const uint64_t n = batch->n_reads;
+  if (!ix->chunk_made) {
+    CU(cudaStreamCreateWithFlags(&ix->h2d, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&ix->d2h, cudaStreamNonBlocking));
+    for (int i = 0; i < mg_index::kMaxChunks; i++) {
+      CU(cudaEventCreateWithFlags(&ix->ev_in[i], cudaEventDisableTiming));
+      CU(cudaEventCreateWithFlags(&ix->ev_done[i], cudaEventDisableTiming));
+    }
+    ix->chunk_made = true;
+  }
+  if (w.chain.alloc(16)) return set_error(MG_ERR_OOM, "chunk counters");
+  cudaStream_t st = ix->stream;
+  const int nc = (int)std::min<uint64_t>(mg_index::kMaxChunks, n / kChunkReads);
+  unsigned long long* chain = w.chain.as<unsigned long long>();
+  CU(cudaMemsetAsync(chain, 0, 16, st));
+  CU(cudaMemcpyAsync(w.offs.p, batch->offsets, (n + 1) * 8, cudaMemcpyHostToDevice, ix->h2d));
+  int rc = MG_OK;
+  for (int i = 0; i < nc && rc == MG_OK; i++) {
+    const uint64_t r0 = n * i / nc, r1 = n * (i + 1) / nc;
+    const uint64_t b0 = batch->offsets[r0], b1 = batch->offsets[r1];
+    if (b1 > b0)
+      CU(cudaMemcpyAsync(w.bases.as<uint8_t>() + b0, batch->bases + b0, b1 - b0, cudaMemcpyHostToDevice, ix->h2d));
+    CU(cudaEventRecord(ix->ev_in[i], ix->h2d));
+    CU(cudaStreamWaitEvent(st, ix->ev_in[i], 0));
+    rc = run_pipeline(ix, w, r1 - r0, w.offs.as<uint64_t>() + r0, w.bases.as<uint8_t>(),
+                      w.reads.as<mg_read_result>() + r0, w.cands.as<mg_candidate>(), out->cand_cap, st, false, chain);
+    if (rc) break;
+    CU(cudaEventRecord(ix->ev_done[i], st));
+    CU(cudaStreamWaitEvent(ix->d2h, ix->ev_done[i], 0));
+    CU(cudaMemcpyAsync(out->reads + r0, w.reads.as<mg_read_result>() + r0, (r1 - r0) * sizeof(mg_read_result),
+                       cudaMemcpyDeviceToHost, ix->d2h));
+  }
+  unsigned long long h[2] = {0, 0};
+  if (rc == MG_OK) CU(cudaMemcpyAsync(h, chain, 16, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(ix->h2d));
+  CU(cudaStreamSynchronize(st));
+  CU(cudaStreamSynchronize(ix->d2h));
+  if (rc) return rc;
+  int err = 0;
+  std::memcpy(&err, &h[1], 4);
+  out->n_cands = h[0];
+  if (err & kErrArena) return kRunWhole;
+  rc = error_status(err);
+  if (rc) return rc;
+  if (h[0]) {
+    CU(cudaMemcpyAsync(out->cands, w.cands.p, h[0] * sizeof(mg_candidate), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  return MG_OK;
+}
+
 static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bool plain) {
   if (!ix || !batch || !out || (batch->n_reads && (!batch->offsets || !batch->bases || !out->reads)))
     return set_error(MG_ERR_INVAL, "null argument");
@@ -642,6 +759,10 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   if (rc) return rc;
   if (w.cands.alloc(std::max<uint64_t>(out->cand_cap, 1) * sizeof(mg_candidate)))
     return set_error(MG_ERR_OOM, "candidate buffer");
+  if (!plain && n >= 2 * kChunkReads) {
+    rc = classify_chunked(ix, w, batch, out);
+    if (rc != kRunWhole) return rc;
+  }
   cudaStream_t st = ix->stream;
   if (n) {
     CU(cudaMemcpyAsync(w.offs.p, batch->offsets, (n + 1) * 8, cudaMemcpyHostToDevice, st));
@@ -738,6 +859,14 @@ void mg_close(mg_index* ix) {
   if (ix->stream) cudaStreamDestroy(ix->stream);
   if (ix->events_made)
     for (auto& e : ix->ev) cudaEventDestroy(e);
+  if (ix->chunk_made) {
+    cudaStreamDestroy(ix->h2d);
+    cudaStreamDestroy(ix->d2h);
+    for (int i = 0; i < mg_index::kMaxChunks; i++) {
+      cudaEventDestroy(ix->ev_in[i]);
+      cudaEventDestroy(ix->ev_done[i]);
+    }
+  }
   delete ix;
 }
 
@@ -803,7 +932,7 @@ int mg_set_timing(mg_index* ix, int on) {
 int mg_last_kernel_times(mg_index* ix, float* ms) {
   if (!ix || !ms) return set_error(MG_ERR_INVAL, "null argument");
   if (!ix->timing || !ix->events_made) return set_error(MG_ERR_INVAL, "timing is off");
-  for (int i = 0; i < 4; i++) {
+  for (int i = 0; i < 5; i++) {
     CU(cudaEventSynchronize(ix->ev[i + 1]));
     CU(cudaEventElapsedTime(&ms[i], ix->ev[i], ix->ev[i + 1]));
   }

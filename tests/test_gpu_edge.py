@@ -131,3 +131,47 @@ def test_many_candidates_grow_staging_arena(tmp_path, form):
     seqs = [core[s:s + 150].tobytes() for s in starts]
     r = check_against_oracle(gix, oix, seqs, form)
     assert (r.reads["n_fwd"] + r.reads["n_rc"]).sum() >= 24 * 5000
+
+
+def _tile(data, offs, times):
+    n, nb = len(offs) - 1, int(offs[-1])
+    o = np.concatenate([offs[:-1].astype(np.uint64) + np.uint64(k * nb) for k in range(times)] +
+                       [np.array([times * nb], np.uint64)])
+    return np.tile(data, times), o
+
+
+def _same(a, b):
+    assert np.array_equal(a.reads.view(np.uint8), b.reads.view(np.uint8))
+    assert np.array_equal(a.cands.view(np.uint8), b.cands.view(np.uint8))
+
+
+def test_chunked_batch_equals_one_piece(golden):
+    """A batch large enough for the chunked form (copies overlapped with classification, candidate
+    offsets continued across chunks) equals the plain form and repeats the golden results."""
+    g = golden("uneven_small")
+    gix = M.Index(g.image)
+    data, offs = _tile(g.reads.data, g.reads.offs, 100)
+    big = gix.classify(data, offs)
+    _same(big, gix.classify(data, offs, form="plain"))
+    one = gix.classify(g.reads.data, g.reads.offs)
+    n = len(g.reads.offs) - 1
+    assert np.array_equal(big.reads[:n]["highest"].view(np.uint32), one.reads["highest"].view(np.uint32))
+    assert np.array_equal(big.reads[-n:]["n_top"], one.reads["n_top"])
+
+
+def test_chunked_batch_staging_overflow_runs_whole(tmp_path):
+    """Every read has 24 candidates: a chunk overflows the staging arena, and the batch is then
+    classified in one piece with a larger arena; the result equals the plain form."""
+    rng = np.random.default_rng(23)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 20000)]
+    refs = [core] * 24 + [acgt[rng.integers(0, 4, 20000)] for _ in range(4)]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    gix = M.Index(M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))]))
+    starts = rng.integers(0, 20000 - 150, 270000)
+    data = np.concatenate([core[s:s + 150] for s in starts])
+    roffs = np.arange(0, 150 * 270001, 150, dtype=np.uint64)
+    a = gix.classify(data, roffs)
+    assert (a.reads["n_fwd"] + a.reads["n_rc"]).sum() >= 24 * 270000
+    _same(a, gix.classify(data, roffs, form="plain"))
