@@ -26,6 +26,8 @@ struct DevIndex {
   const uint32_t* logx_keys;    // sorted float bits of those inputs
   const float* logx_vals;       // host logf at those inputs
   uint32_t n_logx;
+  const float* log_den;         // [lm] logf(scoreMax(lm)) for lm in [0, 65536): the relative
+                                // score's denominator, which depends only on min(qlen, rlen)
 };
 
 // Error word bits set by kernels (first error kept by the host).
@@ -116,6 +118,17 @@ __device__ __forceinline__ float relative_score(const DevIndex& ix, float qlen, 
   const float score_max = __double2float_rn(__dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(lm, __dadd_rn(lm, 1.0)), 2.0), lm), 1.0));
   const float s1 = __fadd_rn(score, 1.0f);
   return __fdiv_rn(ref_logf(ix, s1, err), ref_logf(ix, score_max, err));
+}
+
+// relative_score for integer lengths, the denominator read from ix.log_den (filled at open with
+// the same arithmetic as relative_score, so the result is the same float). min(qlen, rlen) equals
+// the float min of relative_score: qlen < 2^16 is exact, and an rlen that float rounds is > qlen.
+__device__ __forceinline__ float relative_score_tab(const DevIndex& ix, uint32_t qlen, uint32_t rlen, float score,
+                                                    int* err) {
+  const uint32_t lm = qlen < rlen ? qlen : rlen;
+  if (lm == 0 || lm > 0xFFFFu) return relative_score(ix, __uint2float_rn(qlen), __uint2float_rn(rlen), score, err);
+  const float s1 = __fadd_rn(score, 1.0f);
+  return __fdiv_rn(ref_logf(ix, s1, err), __ldg(ix.log_den + lm));
 }
 
 // CalculateScore's final arithmetic (MatrixCPU.cpp:209-212).

@@ -80,7 +80,7 @@ struct mg_index {
   int device = 0;
   mg::DevIndex dix{};
   mg::MhmIndex host;  // refs, headers, taxids kept; postings released after upload
-  mg::DevBuf dir, post, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals;
+  mg::DevBuf dir, post, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals, log_den;
   mg::Workspace ws;   // workspace of the synchronous entry points
   cudaStream_t stream = nullptr;
   // chunked batched form: copy streams and per-chunk events (made on first use)

@@ -110,24 +110,47 @@ struct StageDev {
   unsigned long long* arena_n;
 };
 
-// Dual-strand warp tier: every read of the batch, one warp per read (a half-warp per strand),
-// work stealing in chunks; reads that do not fit go to the lean warp tier.
-__global__ void __launch_bounds__(kW1Warps * 32) k_classify_dual(DevIndex ix, BatchDev b, StageDev sd) {
-  __shared__ DualSmem sm[kW1Warps];
+// Dual-strand warp tiers, one warp per read (a half-warp per strand), work stealing.
+// LIST false: every read of the batch in chunks of kW1Chunk; reads that do not fit go to ovfL.
+// LIST true: the reads of ovfL one at a time; reads that do not fit go to ovf0 (general tier).
+template <int SPL, int SLOTS, int WARPS, bool LIST, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_classify_dual(DevIndex ix, BatchDev b, StageDev sd) {
+  __shared__ DualSmem<SLOTS> sm[WARPS];
+  __shared__ uint8_t comp[256];
+  for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
+  __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  DualSmem& S = sm[w];
-  for (;;) {
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if ((uint64_t)base >= b.n) break;
-    const uint64_t end64 = (uint64_t)base + kW1Chunk;
-    const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
-    for (uint32_t r = base; r < end; r++) {
-      if (!process_read_dual(ix, b, r, S, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+  DualSmem<SLOTS>& S = sm[w];
+  if (!LIST) {
+    for (;;) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if ((uint64_t)base >= b.n) break;
+      const uint64_t end64 = (uint64_t)base + kW1Chunk;
+      const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
+      for (uint32_t r = base; r < end; r++) {
+        if (!process_read_dual<SPL, SLOTS>(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+          if (lane == 0) {
+            unsigned at = atomicAdd(b.n_ovfL, 1u);
+            b.ovfL[at] = r;
+          }
+        }
+        __syncwarp();
+      }
+    }
+  } else {
+    const uint32_t n = *b.n_ovfL;
+    for (;;) {
+      uint32_t item = 0;
+      if (lane == 0) item = atomicAdd(b.workL, 1u);
+      item = __shfl_sync(0xffffffffu, item, 0);
+      if (item >= n) break;
+      const uint32_t r = b.ovfL[item];
+      if (!process_read_dual<SPL, SLOTS>(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
         if (lane == 0) {
-          unsigned at = atomicAdd(b.n_ovfL, 1u);
-          b.ovfL[at] = r;
+          unsigned at = atomicAdd(b.n_ovf0, 1u);
+          b.ovf0[at] = r;
         }
       }
       __syncwarp();
@@ -135,46 +158,7 @@ __global__ void __launch_bounds__(kW1Warps * 32) k_classify_dual(DevIndex ix, Ba
   }
 }
 
-// Lean warp tier over the dual tier's leftovers, one warp per read (one strand after the
-// other on all 32 lanes); reads that do not fit the lean path go to the general warp tier.
-struct LeanSmem {
-  uint32_t a[8][kLeanE];
-  mg_candidate cb[2][kW1C];
-  uint8_t q[kLeanQ];
-};
-
-__global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp(DevIndex ix, BatchDev b, StageDev sd) {
-  __shared__ LeanSmem sm[kW1Warps];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  LeanSmem& S = sm[w];
-  LeanWS lw;
-  lw.e_ref = S.a[0];
-  lw.e_pos = S.a[1];
-  lw.e_fj = S.a[2];
-  lw.s_ref = S.a[3];
-  lw.s_pos = S.a[4];
-  lw.s_j = S.a[5];
-  lw.z = S.a[6];
-  lw.segmax = S.a[7];
-  mg_candidate* const cbs[2] = {S.cb[0], S.cb[1]};
-  const uint32_t n = *b.n_ovfL;
-  for (;;) {
-    uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(b.workL, 1u);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= n) break;
-    const uint32_t r = b.ovfL[item];
-    if (!process_read_lean(ix, b, r, S.q, lw, cbs, kW1C, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
-      if (lane == 0) {
-        unsigned at = atomicAdd(b.n_ovf0, 1u);
-        b.ovf0[at] = r;
-      }
-    }
-    __syncwarp();
-  }
-}
-
-// General warp tier over the lean tier's leftovers; its own leftovers go to the block tier.
+// General warp tier over the dual tiers's leftovers; its own leftovers go to the block tier.
 __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp_list(DevIndex ix, BatchDev b, StageDev sd) {
   __shared__ WarpSmem sm[kW1Warps];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -404,6 +388,17 @@ namespace mg {
 
 // Compare the device log with the host libm logf over the whole domain and record where
 // they differ, so that the device reproduces the reference's logf bit for bit.
+// log_den[lm] = the denominator of relative_score at len_max = lm (its own code, so the values are
+// the ones relative_score computes).
+__global__ void k_fill_log_den(DevIndex ix, float* out) {
+  const uint32_t lm = blockIdx.x * blockDim.x + threadIdx.x;
+  if (lm > 0xFFFFu) return;
+  const double l = (double)__uint2float_rn(lm);
+  const float score_max = __double2float_rn(__dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(l, __dadd_rn(l, 1.0)), 2.0), l), 1.0));
+  int err = 0;
+  out[lm] = ref_logf(ix, score_max, &err);
+}
+
 static int build_log_table(mg_index* ix) {
   const uint32_t chunk = 1u << 23;
   DevBuf dprobe;
@@ -463,6 +458,12 @@ static int build_log_table(mg_index* ix) {
   ix->dix.logx_vals = ix->logx_vals.as<float>();
   ix->dix.n_logx = (uint32_t)keys.size();
   ix->device_bytes += bitmap.size() * 4 + keys.size() * 8;
+  if (ix->log_den.alloc(65536 * 4)) return set_error(MG_ERR_OOM, "log table");
+  k_fill_log_den<<<256, 256, 0, ix->stream>>>(ix->dix, ix->log_den.as<float>());
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(ix->stream));
+  ix->dix.log_den = ix->log_den.as<float>();
+  ix->device_bytes += 65536 * 4;
   return MG_OK;
 }
 
@@ -609,14 +610,14 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       if (tm) CU(cudaEventRecord(ix->ev[2], st));
       if (tm) CU(cudaEventRecord(ix->ev[3], st));
     } else {
-      int per_smd = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_smd, k_classify_dual, kW1Warps * 32, 0);
-      k_classify_dual<<<(unsigned)std::max(1, per_smd) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      auto k1 = k_classify_dual<1, 2, kW1Warps, false, 5>;
+      auto k2 = k_classify_dual<2, 4, kW1Warps / 2, true, 6>;
+      int per_sm1 = 0, per_sm2l = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k1, kW1Warps * 32, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2l, k2, kW1Warps * 16, 0);
+      k1<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
-      int per_sm = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_classify_warp, kW1Warps * 32, 0);
-      unsigned grid = (unsigned)std::max(1, per_sm) * sms;
-      k_classify_warp<<<grid, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      k2<<<(unsigned)std::max(1, per_sm2l) * sms, kW1Warps * 16, 0, st>>>(ix->dix, b, sd);
       int per_sm2 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
       k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
@@ -853,7 +854,7 @@ void mg_close(mg_index* ix) {
   if (!ix) return;
   cudaSetDevice(ix->device);
   for (DevBuf* b : {&ix->dir, &ix->post, &ix->bases, &ix->ref_off, &ix->ref_len, &ix->logx_bitmap, &ix->logx_keys,
-                    &ix->logx_vals})
+                    &ix->logx_vals, &ix->log_den})
     b->release();
   ix->ws.release();
   if (ix->stream) cudaStreamDestroy(ix->stream);
