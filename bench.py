@@ -17,7 +17,7 @@ flush is needed between steps.
   served      the served form (mg_server_*): saturated reads/s with requests of log-uniform
               size in [1, 50000] reads, then p50/p99 request latency under Poisson arrivals at
               25/50/75/90% of that rate.
-  roofline    the warp tiers (two dual-strand kernels and the general warp kernel, which take
+  roofline    the warp tiers (the dual-strand kernel and the general warp kernel, which take
               every read once between them; 97% of a step): algorithmic bytes per step / their CUDA-event
               time, against the measured HBM copy bandwidth.
   cpu_baseline the reference's own CPU path (oracle/_ref harness) when built, else the CPU
@@ -44,9 +44,9 @@ sys.path.insert(0, ROOT)
 
 SEED = 2024
 N_READS = 1_000_000
-# kernels one batched call launches: two dual-strand warp tiers, general warp tier, block tier,
+# kernels one batched call launches: dual-strand warp tier, general warp tier, block tier,
 # global tier, candidate count, scan, scatter
-LAUNCHES_PER_BATCH = 8
+LAUNCHES_PER_BATCH = 7
 
 
 def log(*a):
@@ -554,12 +554,12 @@ def main():
         peaks = measured_peaks()
         hbm = peaks.get("hbm_gbs")
         ab = algorithmic_bytes(ix, reads, n_cands)
-        # the warp tiers (two dual-strand, general) take every read exactly once between them
+        # the warp tiers (dual-strand, general) take every read exactly once between them
         warp_ms = (kernel_ms[0] + kernel_ms[1]) / args.steps
         achieved = ab["bytes"] / (warp_ms / 1000) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm or 6650.0, "unit": "GB/s",
                 "frac": achieved / (hbm or 6650.0), "traffic": None,
-                "kernel": "warp tiers: k_classify_dual<1,2> + k_classify_dual<2,4> + k_classify_warp_list",
+                "kernel": "warp tiers: k_classify_dual + k_classify_warp_list",
                 "kernel_ms": warp_ms,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": ab}
@@ -584,7 +584,7 @@ def main():
                 "batched_over_plain_e2e": e2e / plain,
                 "served": served,
                 "kernel_ms_per_step": {"dual_warp_tier": kernel_ms[0] / args.steps,
-                                       "second_dual_and_general_warp_tiers": kernel_ms[1] / args.steps,
+                                       "general_warp_tier": kernel_ms[1] / args.steps,
                                        "block_tier": kernel_ms[2] / args.steps,
                                        "global_tier": kernel_ms[3] / args.steps,
                                        "compaction": kernel_ms[4] / args.steps},

@@ -248,8 +248,8 @@ class Index:
         _check(lib().mg_set_timing(self.h, 1 if on else 0), "mg_set_timing")
 
     def last_kernel_times(self) -> np.ndarray:
-        """Device ms of the last call: [first dual-strand warp tier or plain kernel, second
-        dual-strand + general warp tiers, block tier, global tier, output compaction]."""
+        """Device ms of the last call: [dual-strand warp tier or plain kernel, general warp tier,
+        block tier, global tier, output compaction]."""
         ms = np.zeros(5, np.float32)
         _check(lib().mg_last_kernel_times(self.h, ms.ctypes.data), "mg_last_kernel_times")
         return ms

@@ -49,9 +49,6 @@ struct BatchDev {
   unsigned long long* n_cands;   // output cursor
   int* err;                      // OR of kErr* bits
   unsigned int* work;            // work-stealing cursor for the dual-strand warp tier
-  uint32_t* ovfL;                // reads handed to the lean warp tier
-  unsigned int* n_ovfL;
-  unsigned int* workL;           // cursor over ovfL
   uint32_t* ovf0;                // reads handed to the general warp tier
   unsigned int* n_ovf0;
   unsigned int* work1;           // cursor over ovf0

@@ -110,44 +110,24 @@ struct StageDev {
   unsigned long long* arena_n;
 };
 
-// Dual-strand warp tiers, one warp per read (a half-warp per strand), work stealing.
-// LIST false: every read of the batch in chunks of kW1Chunk; reads that do not fit go to ovfL.
-// LIST true: the reads of ovfL one at a time; reads that do not fit go to ovf0 (general tier).
-template <int SPL, int SLOTS, int WARPS, bool LIST, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) k_classify_dual(DevIndex ix, BatchDev b, StageDev sd) {
-  __shared__ DualSmem<SLOTS> sm[WARPS];
+// Dual-strand warp tier: every read of the batch, one warp per read (a half-warp per strand),
+// work stealing in chunks of kW1Chunk reads; reads that do not fit go to the general warp tier.
+__global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix, BatchDev b, StageDev sd) {
+  __shared__ DualSmem sm[kW1Warps];
   __shared__ uint8_t comp[256];
   for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  DualSmem<SLOTS>& S = sm[w];
-  if (!LIST) {
-    for (;;) {
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if ((uint64_t)base >= b.n) break;
-      const uint64_t end64 = (uint64_t)base + kW1Chunk;
-      const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
-      for (uint32_t r = base; r < end; r++) {
-        if (!process_read_dual<SPL, SLOTS>(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
-          if (lane == 0) {
-            unsigned at = atomicAdd(b.n_ovfL, 1u);
-            b.ovfL[at] = r;
-          }
-        }
-        __syncwarp();
-      }
-    }
-  } else {
-    const uint32_t n = *b.n_ovfL;
-    for (;;) {
-      uint32_t item = 0;
-      if (lane == 0) item = atomicAdd(b.workL, 1u);
-      item = __shfl_sync(0xffffffffu, item, 0);
-      if (item >= n) break;
-      const uint32_t r = b.ovfL[item];
-      if (!process_read_dual<SPL, SLOTS>(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+  DualSmem& S = sm[w];
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if ((uint64_t)base >= b.n) break;
+    const uint64_t end64 = (uint64_t)base + kW1Chunk;
+    const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
+    for (uint32_t r = base; r < end; r++) {
+      if (!process_read_dual(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
         if (lane == 0) {
           unsigned at = atomicAdd(b.n_ovf0, 1u);
           b.ovf0[at] = r;
@@ -158,7 +138,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_classify_dual(DevIndex ix,
   }
 }
 
-// General warp tier over the dual tiers's leftovers; its own leftovers go to the block tier.
+// General warp tier over the dual tier's leftovers; its own leftovers go to the block tier.
 __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp_list(DevIndex ix, BatchDev b, StageDev sd) {
   __shared__ WarpSmem sm[kW1Warps];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -548,7 +528,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
   }
   if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
       w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
-      w.ovf.alloc(4 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+      w.ovf.alloc(3 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
@@ -556,7 +536,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 }
 
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
-// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovfL | 60 workL
+// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
                         bool plain, unsigned long long* chain) {
@@ -578,9 +558,6 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   b.work3 = (unsigned*)(ctr + 36);
   b.n_ovf0 = (unsigned*)(ctr + 48);
   b.work1 = (unsigned*)(ctr + 52);
-  b.n_ovfL = (unsigned*)(ctr + 56);
-  b.workL = (unsigned*)(ctr + 60);
-  b.ovfL = w.ovf.as<uint32_t>() + 3 * (n + 4);
   b.ovf0 = w.ovf.as<uint32_t>();
   b.ovf1 = w.ovf.as<uint32_t>() + n + 4;
   b.ovf2 = w.ovf.as<uint32_t>() + 2 * (n + 4);
@@ -610,14 +587,10 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       if (tm) CU(cudaEventRecord(ix->ev[2], st));
       if (tm) CU(cudaEventRecord(ix->ev[3], st));
     } else {
-      auto k1 = k_classify_dual<1, 2, kW1Warps, false, 5>;
-      auto k2 = k_classify_dual<2, 4, kW1Warps / 2, true, 6>;
-      int per_sm1 = 0, per_sm2l = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k1, kW1Warps * 32, 0);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2l, k2, kW1Warps * 16, 0);
-      k1<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      int per_sm1 = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_classify_dual, kW1Warps * 32, 0);
+      k_classify_dual<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
-      k2<<<(unsigned)std::max(1, per_sm2l) * sms, kW1Warps * 16, 0, st>>>(ix->dix, b, sd);
       int per_sm2 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
       k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
