@@ -18,8 +18,9 @@ flush is needed between steps.
               size in [1, 50000] reads, then p50/p99 request latency under Poisson arrivals at
               25/50/75/90% of that rate.
   roofline    the warp tiers (the dual-strand kernel and the general warp kernel, which take
-              every read once between them; 97% of a step): algorithmic bytes per step / their CUDA-event
-              time, against the measured HBM copy bandwidth.
+              every read once between them; 97% of a step): algorithmic bytes per step / their
+              CUDA-event time, against the measured HBM copy bandwidth (peak) and against the
+              random 32-byte-sector gather bandwidth measured in the same run (gather_peak).
   cpu_baseline the reference's own CPU path (oracle/_ref harness) when built, else the CPU
               restatement, on a bounded sample with all host threads.
 
@@ -249,146 +250,47 @@ def run_reference_arm(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s: float, clients: int = 4,
+def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s: float, clients: int = 8,
                  fracs=(0.25, 0.5, 0.75, 0.9)):
     """Served form (mg_server_*): saturated throughput, then latency under Poisson arrivals at
-    fractions of it. Requests are contiguous slices of the host reads with log-uniform sizes in
-    [1, 50000] reads. `clients` threads submit and wait through the C ABI, each with its own
-    preallocated result buffers; every submit copies its request from host memory and every wait
-    copies its results out, inside the measurement."""
-    import collections
+    fractions of it. Native client threads (mirage_b200/libmg_loadgen.so) drive the server
+    through the public C ABI: requests are contiguous slices of the host reads with log-uniform
+    sizes in [1, 50000] reads, each submit copies its request from host memory and each wait
+    copies its results into the client's buffers, inside the measurement."""
     import ctypes as C
 
+    class Report(C.Structure):
+        _fields_ = [("reads_per_s", C.c_double), ("requests", C.c_uint64), ("reads", C.c_uint64),
+                    ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("error", C.c_int)]
+
+    LG = C.CDLL(os.path.join(ROOT, "mirage_b200", "libmg_loadgen.so"))
+    LG.mg_loadgen_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, C.c_double, C.c_uint32,
+                                  C.c_double, C.c_int, C.c_uint64, C.POINTER(Report)]
+    bases = np.ascontiguousarray(bases, np.uint8)
+    offs = np.ascontiguousarray(offs, np.uint64)
     n = len(offs) - 1
-    max_req = min(50000, n)
-    L = M.lib()
-    mean_size = (max_req - 1) / np.log(max_req) if max_req > 1 else 1.0
-
-    class Client:
-        def __init__(self, k):
-            self.rng = np.random.default_rng(seed + 1000 * k)
-            self.reads = np.empty(max_req, dtype=M.READ_DTYPE)
-            self.cap = 64 * max_req
-            self.cands = np.empty(self.cap, dtype=M.CAND_DTYPE)
-            self.res = M._Result(self.reads.ctypes.data, self.cands.ctypes.data, self.cap, 0)
-
-        def request(self):
-            size = int(np.exp(self.rng.uniform(0.0, np.log(max_req + 1))))
-            size = max(1, min(size, max_req))
-            st = int(self.rng.integers(0, n - size + 1))
-            o = offs[st:st + size + 1]
-            ob = np.ascontiguousarray(o - o[0])
-            b = bases[int(o[0]):int(o[-1])]
-            return size, M._Batch(size, ob.ctypes.data, b.ctypes.data), (ob, b)
-
-        def submit(self, req):
-            t = C.c_uint64()
-            while True:
-                rc = L.mg_server_submit(sv.h, C.byref(req[1]), C.byref(t))
-                if rc != -9:
-                    break
-                time.sleep(5e-5)  # admission refused: retry (the wait counts toward latency)
-            if rc != 0:
-                raise RuntimeError(f"mg_server_submit: {rc}")
-            return t.value
-
-        def wait(self, ticket):
-            self.res.n_cands = 0
-            rc = L.mg_server_wait(sv.h, ticket, C.byref(self.res), 600000)
-            if rc != 1:
-                raise RuntimeError(f"mg_server_wait: {rc} {L.mg_last_error()}")
-
     sv = M.Server(ix)
-    cl = [Client(k) for k in range(clients)]
+
+    def run(rate: float, secs: float, depth: int, k: int) -> Report:
+        rep = Report()
+        rc = LG.mg_loadgen_run(sv.h, offs.ctypes.data, bases.ctypes.data, n, clients, secs, 50000, rate, depth,
+                               seed + 1000 * k, C.byref(rep))
+        if rc:
+            raise RuntimeError(f"mg_loadgen_run: {rc} {M.lib().mg_last_error()}")
+        return rep
+
     try:
-        for c in cl:  # warm-up
-            for _ in range(4):
-                c.wait(c.submit(c.request()))
-
-        # saturated: each client keeps up to 4 requests outstanding for ~level_s seconds
-        totals = [0] * clients
-
-        def closed(k):
-            c, q = cl[k], collections.deque()
-            t_end = time.perf_counter() + level_s
-            while time.perf_counter() < t_end:
-                req = c.request()
-                q.append(c.submit(req))
-                totals[k] += req[0]
-                if len(q) >= 4:
-                    c.wait(q.popleft())
-            while q:
-                c.wait(q.popleft())
-
-        t0 = time.perf_counter()
-        th = [threading.Thread(target=closed, args=(k,)) for k in range(clients)]
-        for t in th:
-            t.start()
-        for t in th:
-            t.join()
-        sat = sum(totals) / (time.perf_counter() - t0)
-
+        run(0.0, 0.5, 32, 0)  # warm-up
+        sat = run(0.0, level_s, 32, 1)
         levels = []
-        for f in fracs:
-            rate = f * sat / mean_size / clients  # requests per second per client
-            lat, done = [], [0]
-            lock = threading.Lock()
-
-            def open_loop(k):
-                c = cl[k]
-                pending = collections.deque()
-                cv = threading.Condition()
-                fin = [False]
-                mine = []
-
-                def waiter():
-                    while True:
-                        with cv:
-                            while not pending and not fin[0]:
-                                cv.wait()
-                            if not pending:
-                                return
-                            t, arrive, size = pending.popleft()
-                        c.wait(t)
-                        mine.append((time.perf_counter() - arrive, size))
-
-                w = threading.Thread(target=waiter)
-                w.start()
-                t0 = time.perf_counter()
-                arrive = t0
-                while arrive - t0 < level_s:
-                    arrive += c.rng.exponential(1.0 / rate)
-                    now = time.perf_counter()
-                    if arrive > now:
-                        time.sleep(arrive - now)
-                    req = c.request()
-                    t = c.submit(req)
-                    with cv:
-                        pending.append((t, arrive, req[0]))
-                        cv.notify()
-                with cv:
-                    fin[0] = True
-                    cv.notify()
-                w.join()
-                with lock:
-                    lat.extend(x for x, _ in mine)
-                    done[0] += sum(sz for _, sz in mine)
-
-            t0 = time.perf_counter()
-            th = [threading.Thread(target=open_loop, args=(k,)) for k in range(clients)]
-            for t in th:
-                t.start()
-            for t in th:
-                t.join()
-            span = time.perf_counter() - t0
-            ms = np.array(lat) * 1000
-            levels.append({"offered_frac": f, "offered_reads_s": f * sat, "achieved_reads_s": done[0] / span,
-                           "requests": len(lat), "p50_ms": float(np.percentile(ms, 50)),
-                           "p99_ms": float(np.percentile(ms, 99))})
-        return {"saturated": {"value": sat, "unit": "reads/s"},
-                "requests": "log-uniform 1..%d reads, contiguous slices of the batch" % max_req,
-                "clients": clients, "arrivals": "Poisson (one process per client thread)",
-                "seconds_per_level": level_s, "load": levels}
+        for i, f in enumerate(fracs):
+            r = run(f * sat.reads_per_s, level_s, 1, 2 + i)
+            levels.append({"offered_frac": f, "offered_reads_s": f * sat.reads_per_s, "achieved_reads_s": r.reads_per_s,
+                           "requests": int(r.requests), "p50_ms": r.p50_ms, "p99_ms": r.p99_ms, "mean_ms": r.mean_ms})
+        return {"saturated": {"value": sat.reads_per_s, "unit": "reads/s", "p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms},
+                "requests": "log-uniform 1..50000 reads, contiguous slices of the batch",
+                "clients": f"{clients} native threads (libmg_loadgen.so), closed loop 32 deep when saturated",
+                "arrivals": "Poisson (one process per client thread)", "seconds_per_level": level_s, "load": levels}
     finally:
         sv.close()
 
@@ -557,8 +459,12 @@ def main():
         # the warp tiers (dual-strand, general) take every read exactly once between them
         warp_ms = (kernel_ms[0] + kernel_ms[1]) / args.steps
         achieved = ab["bytes"] / (warp_ms / 1000) / 1e9
+        gather = M.gather_bandwidth(local, 4 << 30)
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm or 6650.0, "unit": "GB/s",
                 "frac": achieved / (hbm or 6650.0), "traffic": None,
+                "gather_peak": gather, "frac_of_gather": achieved / gather,
+                "gather_peak_what": "random 32-byte sector gathers, 8 lanes per sector, over a 4 GiB buffer "
+                                    "(mg_gather_bandwidth), measured in this run",
                 "kernel": "warp tiers: k_classify_dual + k_classify_warp_list",
                 "kernel_ms": warp_ms,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6650 GB/s",

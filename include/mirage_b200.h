@@ -121,6 +121,12 @@ int mg_eval_logf(mg_index* ix, const float* x, float* out, uint64_t n);
  * form's kernel), general warp tier, block tier, global-memory tier, output compaction]. mg_bucket_sizes returns the number of postings stored under each of n 28-bit
  * hashes (the index directory, read on the device). */
 int mg_set_timing(mg_index* ix, int on);
+/* Diagnostic (no counterpart in the reference): the roofline of the lookup path. Times 2^26
+ * gathers of whole 32-byte sectors (8 lanes per sector) at pseudo-random positions of a device
+ * buffer of the largest power of two <= buffer_bytes (use several times the L2 size) on
+ * `device`, best of three after a warm-up, and writes the achieved GB/s. Allocates and frees
+ * the buffer itself. */
+int mg_gather_bandwidth(int device, uint64_t buffer_bytes, double* gbs);
 int mg_last_kernel_times(mg_index* ix, float* ms5);
 int mg_bucket_sizes(mg_index* ix, const uint32_t* hashes, uint32_t* counts, uint64_t n);
 

@@ -24,7 +24,7 @@ ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LI
           -6: "MG_ERR_BADINPUT", -7: "MG_ERR_TIMEOUT", -8: "MG_ERR_INVAL", -9: "MG_ERR_BUSY"}
 
 EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
-           "mg_set_timing", "mg_last_kernel_times", "mg_bucket_sizes",
+           "mg_set_timing", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
            "mg_build_image", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_poll",
@@ -89,6 +89,7 @@ def lib() -> C.CDLL:
         L.mg_server_destroy.argtypes = [vp]
         L.mg_server_destroy.restype = None
         L.mg_set_timing.argtypes = [vp, i32]
+        L.mg_gather_bandwidth.argtypes = [i32, u64, C.POINTER(C.c_double)]
         L.mg_last_kernel_times.argtypes = [vp, vp]
         L.mg_bucket_sizes.argtypes = [vp, vp, vp, u64]
         L.mg_inspect_image.argtypes = [vp, u64, i32, C.POINTER(_Info)]
@@ -119,6 +120,13 @@ def _u8(a) -> np.ndarray:
 
 def _u64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def gather_bandwidth(device: int = 0, buffer_bytes: int = 1 << 30) -> float:
+    """Measured random 32-byte-sector gather bandwidth of `device` in GB/s (mg_gather_bandwidth)."""
+    out = C.c_double()
+    _check(lib().mg_gather_bandwidth(device, buffer_bytes, C.byref(out)), "mg_gather_bandwidth")
+    return out.value
 
 
 def build_image(bases, offsets, names, k: int = 31, word: int = 0, taxids=None) -> np.ndarray:

@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmirage_b200.so")
 TOOL = os.path.join(HERE, "mirage_gpu")
+LOADGEN = os.path.join(HERE, "libmg_loadgen.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -23,6 +24,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,
 LIB_SOURCES = ["mg_lib.cu", "mg_server.cu", "mhm.cpp", "mg_output.cu", "mg_noalloc.cu"]
 HEADERS = ["mg_device.cuh", "mg_kernels.cuh", "mg_lean.cuh", "mg_dual.cuh", "mhm.h", "mg_internal.h", "mg_ring.h"]
 TOOL_SOURCES = ["mirage_gpu.cpp"]
+LOADGEN_SOURCES = ["mg_loadgen.cpp"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:
@@ -55,6 +57,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if tsrc and (force or _stale(TOOL, tsrc + [LIB])):
         cmd = ["g++", "-O2", "-std=c++17", "-I", inc, *tsrc, "-o", TOOL, "-L", HERE, "-lmirage_b200",
                "-Wl,-rpath,$ORIGIN", "-lpthread"]
+        subprocess.run(cmd, check=True)
+    lsrc = [os.path.join(CSRC, s) for s in LOADGEN_SOURCES]
+    if force or _stale(LOADGEN, lsrc + [LIB, os.path.join(inc, "mirage_b200.h")]):
+        cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", inc, *lsrc, "-o", LOADGEN, "-L", HERE,
+               "-lmirage_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"]
         subprocess.run(cmd, check=True)
     return LIB
 

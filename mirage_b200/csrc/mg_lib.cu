@@ -921,6 +921,65 @@ __global__ void k_bucket_sizes(const uint32_t* dir, const uint32_t* h, uint32_t*
   }
 }
 
+// Random 32-byte-sector gathers, the access pattern of the directory and posting probes: each
+// group of 8 lanes reads one whole sector (4 bytes per lane, so a warp instruction reads 4
+// sectors) at a pseudo-random sector index (splitmix64 of the gather number, masked to the
+// power-of-two number of sectors), through L2 only, 8 gathers in flight per group.
+__global__ void __launch_bounds__(256) k_gather_sectors(const uint32_t* buf, uint64_t sec_mask, uint64_t n_gathers,
+                                                        unsigned long long* sink) {
+  const uint32_t sub = threadIdx.x & 7;
+  const uint64_t stride = ((uint64_t)gridDim.x * blockDim.x) >> 3;
+  uint32_t acc = 0;
+  for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 3; g < n_gathers; g += 8 * stride) {
+    uint32_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const uint64_t gg = g + u * stride;
+      uint64_t x = gg + 0x9E3779B97F4A7C15ull;
+      x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+      x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+      x ^= x >> 31;
+      const uint64_t s = gg < n_gathers ? (x & sec_mask) : 0;
+      v[u] = __ldcg(buf + 8 * s + sub);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) acc ^= v[u];
+  }
+  if (acc == 0x9E3779B9u) atomicAdd(sink, 1ull);
+}
+
+int mg_gather_bandwidth(int device, uint64_t buffer_bytes, double* gbs) {
+  if (!gbs || buffer_bytes < (1u << 20)) return set_error(MG_ERR_INVAL, "buffer below 1 MiB or null output");
+  CU(cudaSetDevice(device));
+  uint64_t n_sec = 1;
+  while (n_sec * 2 <= buffer_bytes / 32) n_sec *= 2;  // the largest power of two that fits
+  DevBuf buf, sink;
+  if (buf.alloc(n_sec * 32) || sink.alloc(8)) return set_error(MG_ERR_OOM, "gather buffer");
+  CU(cudaMemset(buf.p, 0x5A, n_sec * 32));
+  CU(cudaMemset(sink.p, 0, 8));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const uint64_t n_gathers = 1ull << 26;  // 2 GiB of sectors per launch
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  float best = 0.0f;
+  for (int rep = 0; rep < 4; rep++) {
+    CU(cudaEventRecord(e0, 0));
+    k_gather_sectors<<<(unsigned)sms * 8, 256>>>(buf.as<uint32_t>(), n_sec - 1, n_gathers, sink.as<unsigned long long>());
+    CU(cudaEventRecord(e1, 0));
+    CU(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0 && (best == 0.0f || ms < best)) best = ms;  // the first launch is a warm-up
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CU(cudaGetLastError());
+  *gbs = (double)n_gathers * 32.0 / (best * 1e-3) / 1e9;
+  return MG_OK;
+}
+
 int mg_bucket_sizes(mg_index* ix, const uint32_t* hashes, uint32_t* counts, uint64_t n) {
   if (!ix || (n && (!hashes || !counts))) return set_error(MG_ERR_INVAL, "null argument");
   std::lock_guard<std::mutex> lk(ix->mu);
