@@ -139,6 +139,14 @@ int mg_build_image(const uint8_t* bases, const uint64_t* offsets, uint32_t n_ref
                    uint8_t** image, uint64_t* len);
 void mg_free(void* p);
 
+/* mg_build_image on `device`: the same image, byte for byte, built by GPU kernels (window
+ * hashing, one radix sort by (hash, position), bucket sizing and record encoding; the host lays
+ * out the header, the reference tables and the sequence block). Needs about 64 bytes of device
+ * memory per indexed position. */
+int mg_build_image_device(int device, const uint8_t* bases, const uint64_t* offsets, uint32_t n_refs,
+                          const char* const* names, const int32_t* taxids, int k, int word,
+                          uint8_t** image, uint64_t* len);
+
 /* Plain form. Replaces the reference's per-batch sequence TPrepareGPUAnalysis (Analyser.cpp:
  * 1317) -> CPUGetHighestScore (MatrixCPU.cpp:417) -> strand merge (Analyser.cpp:592-611):
  * one block per read in one launch per batch (the global-memory tier takes reads beyond its

@@ -25,7 +25,7 @@ ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LI
 
 EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
            "mg_set_timing", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
-           "mg_build_image", "mg_free",
+           "mg_build_image", "mg_build_image_device", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_poll",
            "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error", "mg_logs_open", "mg_logs_write",
@@ -74,6 +74,8 @@ def lib() -> C.CDLL:
         L.mg_index_get_info.argtypes = [vp, C.POINTER(_Info)]
         L.mg_build_image.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_char_p), vp, i32, i32,
                                      C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(u64)]
+        L.mg_build_image_device.argtypes = [i32, vp, vp, C.c_uint32, C.POINTER(C.c_char_p), vp, i32, i32,
+                                            C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(u64)]
         L.mg_free.argtypes = [vp]
         L.mg_free.restype = None
         L.mg_score_batch.argtypes = [vp, C.POINTER(_Batch), C.POINTER(_Result)]
@@ -129,8 +131,9 @@ def gather_bandwidth(device: int = 0, buffer_bytes: int = 1 << 30) -> float:
     return out.value
 
 
-def build_image(bases, offsets, names, k: int = 31, word: int = 0, taxids=None) -> np.ndarray:
-    """Build a .mhm image (the reference's index format) from references."""
+def build_image(bases, offsets, names, k: int = 31, word: int = 0, taxids=None, device: int | None = None) -> np.ndarray:
+    """Build a .mhm image (the reference's index format) from references; on the host, or with
+    GPU kernels on `device` (the same bytes)."""
     L = lib()
     bases, offsets = _u8(bases), _u64(offsets)
     n = len(offsets) - 1
@@ -138,9 +141,13 @@ def build_image(bases, offsets, names, k: int = 31, word: int = 0, taxids=None) 
     tax = None if taxids is None else np.ascontiguousarray(taxids, dtype=np.int32)
     out = C.POINTER(C.c_uint8)()
     ln = C.c_uint64()
-    _check(L.mg_build_image(bases.ctypes.data, offsets.ctypes.data, n, arr,
-                            None if tax is None else tax.ctypes.data, k, word, C.byref(out), C.byref(ln)),
-           "mg_build_image")
+    if device is None:
+        rc = L.mg_build_image(bases.ctypes.data, offsets.ctypes.data, n, arr, None if tax is None else tax.ctypes.data,
+                              k, word, C.byref(out), C.byref(ln))
+    else:
+        rc = L.mg_build_image_device(device, bases.ctypes.data, offsets.ctypes.data, n, arr,
+                                     None if tax is None else tax.ctypes.data, k, word, C.byref(out), C.byref(ln))
+    _check(rc, "mg_build_image")
     try:
         return np.ctypeslib.as_array(out, shape=(ln.value,)).copy()
     finally:

@@ -256,6 +256,119 @@ struct Group {
   uint32_t hash;
 };
 
+int mhm_width_of(uint64_t v) { return width_of(v); }
+
+int mhm_plan(const uint64_t* offs, uint32_t n_refs, const std::vector<std::string>& headers, int word,
+             uint64_t ng, uint64_t rec_total, uint64_t last_rec, MhmPlan* plan, std::string* err) {
+  uint64_t seq_chars = offs[n_refs] - offs[0], hdr_chars = 0;
+  for (uint32_t r = 0; r < n_refs; r++) hdr_chars += headers[r].size() + 2;  // '>' + name + NUL
+  const uint64_t ml = sizeof(kMagic) - 1;
+  auto layout = [&](uint64_t W, uint64_t* toc_at) {
+    uint64_t sp = ml + 8 + 4 + 4 + 4 + 4;
+    *toc_at = sp;
+    sp += ng * W * 2;
+    sp += W + W + n_refs * W + W + n_refs * W + W;
+    sp += W + n_refs * 4ull + n_refs * W + n_refs * W;
+    sp += seq_chars + hdr_chars;
+    return sp;  // the first record
+  };
+  uint64_t toc_at;
+  if (word == 0) word = (layout(4, &toc_at) + rec_total > 0xFFFFFFFFull) ? 8 : 4;
+  if (word != 4 && word != 8) {
+    if (err) *err = "word must be 4 or 8";
+    return MHM_ERR_LIMIT;
+  }
+  plan->W = (uint64_t)word;
+  plan->first_rec = layout(plan->W, &plan->toc_at);
+  plan->total = plan->first_rec + rec_total;
+  // the 32-bit build refuses files whose positions pass 2^32-1 (Hashmap.cpp:2103-2109)
+  if (plan->W == 4 && plan->total - last_rec > 0xFFFFFFFFull) {
+    if (err) *err = "file too large for the 32-bit format; use word 8";
+    return MHM_ERR_LIMIT;
+  }
+  return MHM_OK;
+}
+
+int mhm_write_head(uint8_t* b, const MhmPlan& plan, const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
+                   const std::vector<std::string>& headers, const std::vector<int32_t>& taxids, int k, uint64_t ng,
+                   uint32_t max_group, std::string* err) {
+  const uint64_t W = plan.W;
+  const int Wi = (int)W;
+  uint64_t max_ref = 0, max_hdr = 0;
+  for (uint32_t r = 0; r < n_refs; r++) {
+    max_hdr = std::max<uint64_t>(max_hdr, headers[r].size() + 2);
+    max_ref = std::max<uint64_t>(max_ref, offs[r + 1] - offs[r]);
+  }
+  const uint64_t ml = sizeof(kMagic) - 1;
+  uint64_t o = 0;
+  std::memcpy(b, kMagic, ml);
+  o = ml;
+  wr(b + o, ng, 8);
+  o += 8;
+  wr(b + o, kVersion, 4);
+  wr(b + o + 4, W, 4);
+  wr(b + o + 8, (uint64_t)(uint32_t)k, 4);
+  o += 12;
+  b[o] = (uint8_t)W;
+  b[o + 1] = (uint8_t)width_of(max_group);
+  b[o + 2] = (uint8_t)width_of(max_ref);
+  b[o + 3] = (uint8_t)width_of(max_hdr);
+  o += 4;
+  if (o != plan.toc_at) {
+    if (err) *err = "internal layout mismatch";
+    return MHM_ERR_FORMAT;
+  }
+  o += ng * 2 * W;  // bucket TOC: written by the caller
+  wr(b + o, n_refs, Wi);
+  o += W;
+  for (uint32_t r = 0; r < n_refs; r++) wr(b + o + 4ull * r, (uint32_t)(r < taxids.size() ? taxids[r] : -1), 4);
+  o += 4ull * n_refs;
+  // sequence TOC
+  uint64_t seq_chars = offs[n_refs] - offs[0];
+  uint64_t after = o + W + W + n_refs * W + n_refs * W;
+  const uint64_t seq_start = after + W + W + n_refs * W + n_refs * W;
+  wr(b + o, after, Wi);
+  wr(b + o + W, n_refs, Wi);
+  o += 2 * W;
+  for (uint32_t r = 0; r < n_refs; r++) wr(b + o + W * r, offs[r + 1] - offs[r], Wi);
+  o += W * n_refs;
+  uint64_t spx = seq_start;
+  for (uint32_t r = 0; r < n_refs; r++) {
+    wr(b + o + W * r, spx, Wi);
+    spx += offs[r + 1] - offs[r];
+  }
+  o += W * n_refs;
+  // header TOC
+  after = o + W + W + n_refs * W + n_refs * W;
+  wr(b + o, after, Wi);
+  wr(b + o + W, n_refs, Wi);
+  o += 2 * W;
+  for (uint32_t r = 0; r < n_refs; r++) wr(b + o + W * r, headers[r].size() + 2, Wi);
+  o += W * n_refs;
+  for (uint32_t r = 0; r < n_refs; r++) {
+    wr(b + o + W * r, spx, Wi);
+    spx += headers[r].size() + 2;
+  }
+  o += W * n_refs;
+  if (o != seq_start) {
+    if (err) *err = "internal layout mismatch";
+    return MHM_ERR_FORMAT;
+  }
+  std::memcpy(b + o, bases + offs[0], seq_chars);
+  o += seq_chars;
+  for (uint32_t r = 0; r < n_refs; r++) {
+    b[o++] = '>';
+    std::memcpy(b + o, headers[r].data(), headers[r].size());
+    o += headers[r].size();
+    b[o++] = 0;
+  }
+  if (o != plan.first_rec) {
+    if (err) *err = "internal layout mismatch";
+    return MHM_ERR_FORMAT;
+  }
+  return MHM_OK;
+}
+
 int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
               const std::vector<std::string>& headers, const std::vector<int32_t>& taxids, int k,
               int word, int nthreads, std::vector<uint8_t>* out, std::string* err) {
@@ -433,108 +546,29 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
   if (too_wide) return fail(MHM_ERR_LIMIT, "a bucket has more distinct positions than its width can count");
   phase("sized");
   // 4. layout and stream positions (SaveHashmapTableV3, Hashmap.cpp:1868-2128)
-  uint64_t seq_chars = offs[n_refs] - offs[0], hdr_chars = 0, max_ref = 0, max_hdr = 0;
-  for (uint32_t r = 0; r < n_refs; r++) {
-    uint64_t hl = headers[r].size() + 2;  // '>' + name + NUL, as the parser stores it
-    hdr_chars += hl;
-    max_hdr = std::max(max_hdr, hl);
-    max_ref = std::max<uint64_t>(max_ref, offs[r + 1] - offs[r]);
-  }
-  const uint64_t ml = sizeof(kMagic) - 1;
-  auto layout = [&](uint64_t W, uint64_t* first_rec) {
-    uint64_t sp = ml + 8 + 4 + 4 + 4 + 4;
-    sp += ng * W * 2;
-    sp += W + W + n_refs * W + W + n_refs * W + W;
-    sp += W + n_refs * 4ull + n_refs * W + n_refs * W;
-    uint64_t seq_start = sp;
-    sp += seq_chars + hdr_chars;
-    *first_rec = sp;
-    return seq_start;
-  };
   uint64_t rec_total = 0;
   for (uint64_t g = 0; g < ng; g++) rec_total += rec_size[g];
-  if (word == 0) {
-    uint64_t fr;
-    layout(4, &fr);
-    word = (fr + rec_total > 0xFFFFFFFFull) ? 8 : 4;
-  }
-  if (word != 4 && word != 8) return fail(MHM_ERR_LIMIT, "word must be 4 or 8");
-  const uint64_t W = (uint64_t)word;
-  uint64_t first_rec;
-  uint64_t seq_start = layout(W, &first_rec);
-  const uint64_t total = first_rec + rec_total;
-  // the 32-bit build refuses files whose positions pass 2^32-1 (Hashmap.cpp:2103-2109)
-  if (W == 4 && total - (ng ? rec_size[ng - 1] : 0) > 0xFFFFFFFFull)
-    return fail(MHM_ERR_LIMIT, "file too large for the 32-bit format; use word 8");
+  MhmPlan plan;
+  int prc = mhm_plan(offs, n_refs, headers, word, ng, rec_total, ng ? rec_size[ng - 1] : 0, &plan, err);
+  if (prc) return prc;
+  const uint64_t W = plan.W;
   phase("planned");
   try {
-    out->assign(total, 0);
+    out->assign(plan.total, 0);
   } catch (...) {
     return fail(MHM_ERR_OOM, "out of host memory for the image");
   }
   phase("allocated");
   uint8_t* b = out->data();
-  uint64_t o = 0;
-  std::memcpy(b, kMagic, ml);
-  o = ml;
-  wr(b + o, ng, 8);
-  o += 8;
-  wr(b + o, kVersion, 4);
-  wr(b + o + 4, W, 4);
-  wr(b + o + 8, (uint64_t)(uint32_t)k, 4);
-  o += 12;
-  b[o] = (uint8_t)W;
-  b[o + 1] = (uint8_t)width_of(max_group);
-  b[o + 2] = (uint8_t)width_of(max_ref);
-  b[o + 3] = (uint8_t)width_of(max_hdr);
-  o += 4;
+  prc = mhm_write_head(b, plan, bases, offs, n_refs, headers, taxids, k, ng, max_group, err);
+  if (prc) return prc;
   std::vector<uint64_t> rec_sp(ng + 1);
-  rec_sp[0] = first_rec;
+  rec_sp[0] = plan.first_rec;
   for (uint64_t g = 0; g < ng; g++) rec_sp[g + 1] = rec_sp[g] + rec_size[g];
-  for (uint64_t g = 0; g < ng; g++) {
-    wr(b + o, groups[g].hash, W);
-    wr(b + o + W, rec_sp[g], W);
-    o += 2 * W;
+  for (uint64_t g = 0, o = plan.toc_at; g < ng; g++, o += 2 * W) {
+    wr(b + o, groups[g].hash, (int)W);
+    wr(b + o + W, rec_sp[g], (int)W);
   }
-  wr(b + o, n_refs, W);
-  o += W;
-  for (uint32_t r = 0; r < n_refs; r++) wr(b + o + 4ull * r, (uint32_t)(r < taxids.size() ? taxids[r] : -1), 4);
-  o += 4ull * n_refs;
-  // sequence TOC
-  uint64_t after = o + W + W + n_refs * W + n_refs * W;
-  wr(b + o, after, W);
-  wr(b + o + W, n_refs, W);
-  o += 2 * W;
-  for (uint32_t r = 0; r < n_refs; r++) wr(b + o + W * r, offs[r + 1] - offs[r], W);
-  o += W * n_refs;
-  uint64_t spx = seq_start;
-  for (uint32_t r = 0; r < n_refs; r++) {
-    wr(b + o + W * r, spx, W);
-    spx += offs[r + 1] - offs[r];
-  }
-  o += W * n_refs;
-  // header TOC
-  after = o + W + W + n_refs * W + n_refs * W;
-  wr(b + o, after, W);
-  wr(b + o + W, n_refs, W);
-  o += 2 * W;
-  for (uint32_t r = 0; r < n_refs; r++) wr(b + o + W * r, headers[r].size() + 2, W);
-  o += W * n_refs;
-  for (uint32_t r = 0; r < n_refs; r++) {
-    wr(b + o + W * r, spx, W);
-    spx += headers[r].size() + 2;
-  }
-  o += W * n_refs;
-  if (o != seq_start) return fail(MHM_ERR_FORMAT, "internal layout mismatch");
-  std::memcpy(b + o, bases + offs[0], seq_chars);
-  o += seq_chars;
-  for (uint32_t r = 0; r < n_refs; r++) {
-    b[o++] = '>';
-    std::memcpy(b + o, headers[r].data(), headers[r].size());
-    o += headers[r].size();
-    b[o++] = 0;
-  }
-  if (o != first_rec) return fail(MHM_ERR_FORMAT, "internal layout mismatch");
   phase("laid out");
   // 5. posting records (Hashmap.cpp:2303-2512)
   parallel_for(ng, std::max(1, nthreads), [&](uint64_t lo, uint64_t hi, int) {

@@ -63,4 +63,23 @@ int mhm_build(const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
 
 uint32_t hash28(const uint8_t* p, int len);
 
+// Byte width of a value in the writer's rule ((bits - 1) / 8) + 1 (Hashmap.cpp:1641-1671).
+int mhm_width_of(uint64_t v);
+
+// Word width and section offsets of a .mhm image with ng buckets whose records take rec_total
+// bytes, the last bucket's last_rec of them (the layout of SaveHashmapTableV3,
+// Hashmap.cpp:1868-2128). word 0 picks 4 unless the file needs 64-bit positions.
+struct MhmPlan {
+  uint64_t W = 0;          // word width, 4 or 8
+  uint64_t toc_at = 0;     // bucket TOC: ng x (hash, record stream position), W bytes each
+  uint64_t first_rec = 0;  // first posting record
+  uint64_t total = 0;      // image size
+};
+int mhm_plan(const uint64_t* offs, uint32_t n_refs, const std::vector<std::string>& headers, int word,
+             uint64_t ng, uint64_t rec_total, uint64_t last_rec, MhmPlan* plan, std::string* err);
+// Everything of the image but the bucket TOC and the records, into out[0, plan.first_rec).
+int mhm_write_head(uint8_t* out, const MhmPlan& plan, const uint8_t* bases, const uint64_t* offs, uint32_t n_refs,
+                   const std::vector<std::string>& headers, const std::vector<int32_t>& taxids, int k, uint64_t ng,
+                   uint32_t max_group, std::string* err);
+
 }  // namespace mg
