@@ -212,7 +212,12 @@ int main(int argc, char** argv) {
     for (auto& n : names) np.push_back(n.c_str());
     uint8_t* img = nullptr;
     uint64_t len = 0;
-    rc = mg_build_image(refs.bases.data(), refs.offs.data(), (uint32_t)names.size(), np.data(), nullptr, k, 0, &img, &len);
+    // on the GPU; the host builder writes the same bytes when the device lacks the memory
+    rc = mg_build_image_device(gpu, refs.bases.data(), refs.offs.data(), (uint32_t)names.size(), np.data(), nullptr, k,
+                               0, &img, &len);
+    if (rc == MG_ERR_OOM)
+      rc = mg_build_image(refs.bases.data(), refs.offs.data(), (uint32_t)names.size(), np.data(), nullptr, k, 0, &img,
+                          &len);
     if (rc) die("building the hashmap", rc);
     if (save_db) {
       std::string p = std::string(dir) + "/hashmap_" + base_name_no_ext(reference) + ".mhm";
