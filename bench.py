@@ -166,6 +166,11 @@ def algorithmic_bytes(ix, reads, n_cands: int, k: int = 31) -> dict:
             "ref_windows": 64 * n_cands, "results": 16 * (len(lens) + n_cands), "seeds": n_seeds}
 
 
+def mhm_word(img: np.ndarray) -> int:
+    """The .mhm word width (4 or 8): the 32-bit field 12 bytes after the 73-byte magic text."""
+    return int.from_bytes(img[85:89].tobytes(), "little")
+
+
 def make_workload(scale: float, n_reads: int, rank: int):
     from mirage_b200 import synth
 
@@ -210,7 +215,7 @@ def run_reference_arm(args, rank: int, world: int) -> None:
 
     refs, reads = make_workload(args.scale, args.reads, 0)
     img = M.build_image(refs.data, refs.offs, refs.headers, k=31)
-    word = int(img[74 + 12])  # the .mhm word width byte
+    word = mhm_word(img)
     threads = os.cpu_count() or 1
     per_step = args.ref_sample
     harness = O.HARNESS if word == 4 else O.HARNESS + "64"
@@ -335,7 +340,7 @@ def main():
     t0 = time.time()
     img = M.build_image(refs.data, refs.offs, refs.headers, k=31, device=local)  # same bytes as the host build
     t_build = time.time() - t0
-    word = int(img[74 + 12])
+    word = mhm_word(img)
     t0 = time.time()
     ix = M.Index(img, k=31, device=local)
     t_open = time.time() - t0

@@ -2,6 +2,8 @@
 // (warp tier, block tier, global-memory tier), output compaction and the host entry points.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -9,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -299,6 +302,124 @@ __global__ void k_fill_dir(const uint32_t* toc_hash, const uint32_t* toc_start, 
   for (uint64_t h = lo; h <= hi; h++) dir[h] = v;
 }
 
+// The posting records of a .mhm image decoded on the device, with the host reader's checks
+// (mhm_parse; the reference's reader Hashmap.cpp:402-580 and decode Analyser.cpp:1602-1752).
+enum : int { kDecHash = 1, kDecOrder = 2, kDecRecord = 4 };
+
+__device__ __forceinline__ uint64_t rd_img(const uint8_t* p, int w) {
+  uint64_t v = 0;
+  for (int i = 0; i < w; i++) v |= (uint64_t)p[i] << (8 * i);
+  return v;
+}
+
+// Bucket TOC: hash and record stream position of every bucket.
+__global__ void k_mhm_toc(const uint8_t* img, uint64_t toc_at, uint64_t n, int W, uint32_t* hash, uint64_t* sp,
+                          int* err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint8_t* p = img + toc_at + i * 2 * (uint64_t)W;
+    uint64_t h = rd_img(p, W);
+    if (h > 0x0FFFFFFFull) {
+      atomicOr(err, kDecHash);
+      h = 0;
+    }
+    hash[i] = (uint32_t)h;
+    sp[i] = rd_img(p + W, W);
+  }
+}
+
+// Postings per bucket (numIDs of its record). The last bucket gets none: the reader stores its
+// BufferSize one past the array (Hashmap.cpp:552-553), so it is present with no postings.
+__global__ void k_mhm_count(const uint8_t* img, uint64_t L, const uint32_t* hash, const uint64_t* sp, uint64_t n,
+                            uint64_t* cnt, int* err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    if (i > 0 && hash[i] <= hash[i - 1]) atomicOr(err, kDecOrder);
+    uint64_t c = 0;
+    if (i + 1 < n) {
+      if (sp[i] >= L || sp[i + 1] <= sp[i]) {
+        atomicOr(err, kDecRecord);
+      } else {
+        const uint8_t* p = img + sp[i];
+        const uint64_t rem = L - sp[i];
+        const uint32_t wo = rem >= 4 ? p[0] : 0, wnum = rem >= 4 ? p[3] : 0;
+        if (rem < 4 || wnum > 8 || wnum < 1 || 4ull + 2ull * wo + wnum > rem) {
+          atomicOr(err, kDecRecord);
+        } else {
+          c = rd_img(p + 4 + 2 * wo, (int)wnum);
+          // widths are at least one byte: no more postings than bytes left (bounds the sum)
+          if (c > rem || c > 0xFFFFFFFFull) {
+            atomicOr(err, kDecRecord);
+            c = 0;
+          }
+        }
+      }
+    }
+    cnt[i] = c;
+  }
+}
+
+__global__ void k_mhm_decode(const uint8_t* img, uint64_t L, const uint64_t* sp, const uint64_t* cnt,
+                             const uint64_t* start, uint64_t n, int word, uint32_t n_refs, uint2* post, int* err) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t M = word >= 8 ? ~0ull : ((1ull << (8 * word)) - 1ull);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t num = cnt[i];
+    if (!num) continue;
+    const uint8_t* p = img + sp[i];
+    uint64_t rem = L - sp[i];
+    const int wo = p[0], wid = p[1], wpos = p[2], wnum = p[3];
+    bool bad = wo > word || wid > word || wpos > word || wo < 1 || wid < 1 || wpos < 1;
+    uint2* out = post + start[i];
+    if (!bad) {
+      const uint64_t id_min = rd_img(p + 4, wo), pos_min = rd_img(p + 4 + wo, wo);
+      const uint64_t hdr = 4ull + 2ull * wo + wnum;
+      p += hdr;
+      rem -= hdr;
+      bad = (wid && num > (rem - 1 - wpos) / wid) || rem < 1ull + wpos + (uint64_t)wid * num;
+      if (!bad) {
+        for (uint64_t j = 0; j < num && !bad; j++) {
+          const uint64_t id = (rd_img(p + j * wid, wid) + id_min) & M;  // "raise" of Analyser.cpp:1666-1686
+          bad = id >= n_refs;
+          out[j].x = (uint32_t)id;
+        }
+        p += (uint64_t)wid * num;
+        rem -= (uint64_t)wid * num;
+        const int wrep = p[0];
+        const uint64_t nrep = rd_img(p + 1, wpos);
+        p += 1 + wpos;
+        rem -= 1 + wpos;
+        bad = bad || wrep > word || wrep < 1 || nrep > num || nrep > rem / (uint64_t)(wrep + wpos);
+        uint64_t filled = 0;
+        for (uint64_t r = 0; r < nrep && !bad; r++) {
+          const uint64_t c = rd_img(p, wrep);
+          const uint64_t v = (rd_img(p + wrep, wpos) + pos_min) & M;
+          p += wrep + wpos;
+          if (filled + c > num || c > num || v > 0xFFFFFFFFull) {
+            bad = true;
+            break;
+          }
+          for (uint64_t t = 0; t < c; t++) out[filled + t].y = (uint32_t)v;
+          filled += c;
+        }
+        bad = bad || filled != num;  // the reference pairs vSeqIDs[k] with vPos[k]
+      }
+    }
+    if (bad) atomicOr(err, kDecRecord);
+  }
+}
+
+// Directory from the ascending TOC and 64-bit bucket starts (values below 2^32).
+__global__ void k_fill_dir64(const uint32_t* toc_hash, const uint64_t* toc_start, uint64_t n, uint32_t total,
+                             uint32_t* dir) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  const uint64_t lo = i == 0 ? 0 : (uint64_t)toc_hash[i - 1] + 1;
+  const uint64_t hi = i == n ? (1ull << 28) : (uint64_t)toc_hash[i];
+  const uint32_t v = i == n ? total : (uint32_t)toc_start[i];
+  for (uint64_t h = lo; h <= hi; h++) dir[h] = v;
+}
+
 __global__ void k_log_probe(uint32_t lo_bits, uint32_t n, float* out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = log_dev_raw(__uint_as_float(lo_bits + i));
@@ -447,39 +568,70 @@ static int build_log_table(mg_index* ix) {
   return MG_OK;
 }
 
-static int upload_index(mg_index* ix, int k) {
+// The HBM index from a .mhm image: the host parses the header and reference tables; the image
+// is copied to the device once and the bucket TOC and posting records are decoded there.
+static int upload_index_image(mg_index* ix, const uint8_t* image, uint64_t L, const MhmMeta& meta, int k) {
   MhmIndex& h = ix->host;
   const uint64_t n = h.n_hash;
-  const uint64_t total = h.postings.size();
-  if (total >= 0xFFFFFFFFull) return set_error(MG_ERR_LIMIT, "more than 2^32-1 postings");
-  // the directory needs the TOC ascending (the builder writes it so); reject duplicates
-  for (uint64_t i = 1; i < n; i++)
-    if (h.toc_hash[i] <= h.toc_hash[i - 1]) return set_error(MG_ERR_BADFMT, "TOC hashes not strictly ascending");
   CU(cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking));
-  if (ix->dir.alloc(((1ull << 28) + 1) * 4) || ix->post.alloc(total * 8 + 8) || ix->bases.alloc(h.bases.size() + 64) ||
+  cudaStream_t st = ix->stream;
+  DevBuf img, dhash, dsp, dcnt, dstart, derr, tmp;
+  if (img.alloc(L + 16) || dhash.alloc(n * 4 + 4) || dsp.alloc(n * 8 + 8) || dcnt.alloc(n * 8 + 8) ||
+      dstart.alloc(n * 8 + 8) || derr.alloc(4))
+    return set_error(MG_ERR_OOM, "device memory for the index image");
+  CU(cudaMemcpy(img.p, image, L, cudaMemcpyHostToDevice));
+  CU(cudaMemsetAsync(derr.p, 0, 4, st));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
+  const unsigned grid = (unsigned)sms * 8;
+  uint64_t total = 0;
+  int err = 0;
+  if (n) {
+    k_mhm_toc<<<grid, 256, 0, st>>>(img.as<uint8_t>(), meta.toc_at, n, h.word, dhash.as<uint32_t>(),
+                                     dsp.as<uint64_t>(), derr.as<int>());
+    k_mhm_count<<<grid, 256, 0, st>>>(img.as<uint8_t>(), L, dhash.as<uint32_t>(), dsp.as<uint64_t>(), n,
+                                       dcnt.as<uint64_t>(), derr.as<int>());
+    CU(cudaGetLastError());
+    size_t tb = 0;
+    CU(cub::DeviceScan::ExclusiveSum(nullptr, tb, dcnt.as<uint64_t>(), dstart.as<uint64_t>(), (int64_t)n, st));
+    if (tmp.alloc(tb + 16)) return set_error(MG_ERR_OOM, "device memory for the index scan");
+    CU(cub::DeviceScan::ExclusiveSum(tmp.p, tb, dcnt.as<uint64_t>(), dstart.as<uint64_t>(), (int64_t)n, st));
+    uint64_t ls = 0, lc = 0;
+    CU(cudaMemcpyAsync(&ls, dstart.as<uint64_t>() + n - 1, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(&lc, dcnt.as<uint64_t>() + n - 1, 8, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(&err, derr.p, 4, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    total = ls + lc;
+    if (err & kDecHash) return set_error(MG_ERR_BADFMT, "hash wider than 28 bits");
+    if (err & kDecRecord) return set_error(MG_ERR_BADFMT, "malformed posting record");
+    if (err & kDecOrder) return set_error(MG_ERR_BADFMT, "TOC hashes not strictly ascending");
+  }
+  if (total >= 0xFFFFFFFFull) return set_error(MG_ERR_LIMIT, "more than 2^32-1 postings");
+  if (ix->dir.alloc(((1ull << 28) + 1) * 4) || ix->post.alloc(total * 8 + 8) || ix->bases.alloc(meta.bases_len + 64) ||
       ix->ref_off.alloc(h.ref_off.size() * 8 + 8) || ix->ref_len.alloc(h.ref_len.size() * 4 + 4))
     return set_error(MG_ERR_OOM, "device allocation for the index");
   ix->device_bytes += ix->dir.n + ix->post.n + ix->bases.n + ix->ref_off.n + ix->ref_len.n;
-  CU(cudaMemcpy(ix->post.p, h.postings.data(), total * 8, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ix->bases.p, h.bases.data(), h.bases.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ix->ref_off.p, h.ref_off.data(), h.ref_off.size() * 8, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ix->ref_len.p, h.ref_len.data(), h.ref_len.size() * 4, cudaMemcpyHostToDevice));
-  {
-    std::vector<uint32_t> start(n);
-    for (uint64_t i = 0; i < n; i++) start[i] = (uint32_t)h.bucket[i];
-    DevBuf dh, ds;
-    if (dh.alloc(n * 4 + 4) || ds.alloc(n * 4 + 4)) return set_error(MG_ERR_OOM, "directory build");
-    if (n) {
-      CU(cudaMemcpy(dh.p, h.toc_hash.data(), n * 4, cudaMemcpyHostToDevice));
-      CU(cudaMemcpy(ds.p, start.data(), n * 4, cudaMemcpyHostToDevice));
-    }
-    k_fill_dir<<<(unsigned)((n + 1 + 255) / 256), 256, 0, ix->stream>>>(dh.as<uint32_t>(), ds.as<uint32_t>(), n,
-                                                                     (uint32_t)total, ix->dir.as<uint32_t>());
+  if (n) {
+    k_mhm_decode<<<grid, 256, 0, st>>>(img.as<uint8_t>(), L, dsp.as<uint64_t>(), dcnt.as<uint64_t>(),
+                                        dstart.as<uint64_t>(), n, h.word, h.n_refs, ix->post.as<uint2>(),
+                                        derr.as<int>());
     CU(cudaGetLastError());
-    CU(cudaStreamSynchronize(ix->stream));
-    dh.release();
-    ds.release();
   }
+  if (meta.bases_len)
+    CU(cudaMemcpyAsync(ix->bases.p, img.as<uint8_t>() + meta.bases_at, meta.bases_len, cudaMemcpyDeviceToDevice, st));
+  CU(cudaMemcpyAsync(ix->ref_off.p, h.ref_off.data(), h.ref_off.size() * 8, cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ix->ref_len.p, h.ref_len.data(), h.ref_len.size() * 4, cudaMemcpyHostToDevice, st));
+  k_fill_dir64<<<(unsigned)((n + 1 + 255) / 256), 256, 0, st>>>(dhash.as<uint32_t>(), dstart.as<uint64_t>(), n,
+                                                                 (uint32_t)total, ix->dir.as<uint32_t>());
+  CU(cudaGetLastError());
+  uint32_t last_hash = 0;
+  if (n) CU(cudaMemcpyAsync(&last_hash, dhash.as<uint32_t>() + n - 1, 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(&err, derr.p, 4, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  if (err & kDecRecord) return set_error(MG_ERR_BADFMT, "malformed posting record");
+  h.has_empty_last = n > 0;
+  h.empty_last_hash = last_hash;
+  ix->info.n_postings = total;
   DevIndex& d = ix->dix;
   d.dir = ix->dir.as<uint32_t>();
   d.post = ix->post.as<uint2>();
@@ -491,24 +643,27 @@ static int upload_index(mg_index* ix, int k) {
   d.k = k;
   d.step = k / 2;
   d.hlen = k - k / 2 + 1;
-  int rc = build_log_table(ix);
-  if (rc) return rc;
-  std::vector<Posting>().swap(h.postings);
-  std::vector<uint8_t>().swap(h.bases);
-  return MG_OK;
+  return build_log_table(ix);
 }
 
-static int open_common(mg_index* ix, int k, int device) {
+static int open_image(mg_index* ix, const uint8_t* image, uint64_t L, int k, int device) {
   ix->device = device;
   CU(cudaSetDevice(device));
+  std::string err;
+  MhmMeta meta;
   auto t0 = std::chrono::steady_clock::now();
-  int rc = upload_index(ix, k);
+  int rc = mhm_parse_meta(image, L, k, &ix->host, &meta, false, &err);
+  if (rc != MHM_OK)
+    return set_error(rc == MHM_ERR_IO ? MG_ERR_IO : rc == MHM_ERR_OOM ? MG_ERR_OOM : rc == MHM_ERR_LIMIT ? MG_ERR_LIMIT : MG_ERR_BADFMT, err);
   auto t1 = std::chrono::steady_clock::now();
-  ix->info.upload_seconds = std::chrono::duration<double>(t1 - t0).count();
+  ix->info.load_seconds += std::chrono::duration<double>(t1 - t0).count();
+  rc = upload_index_image(ix, image, L, meta, k);
+  ix->info.upload_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
   ix->info.k = k;
   ix->info.word = ix->host.word;
   ix->info.n_hashes = ix->host.n_hash;
   ix->info.n_refs = ix->host.n_refs;
+  ix->info.ref_bases = meta.bases_len;
   ix->info.device_bytes = ix->device_bytes;
   return rc;
 }
@@ -785,14 +940,24 @@ const char* mg_strerror(int code) {
   }
 }
 
-static int open_from(mg_index* ix, int rc, const std::string& err, int k, int device, mg_index** out) {
-  if (rc != MHM_OK) {
-    delete ix;
-    return set_error(rc == MHM_ERR_IO ? MG_ERR_IO : rc == MHM_ERR_OOM ? MG_ERR_OOM : rc == MHM_ERR_LIMIT ? MG_ERR_LIMIT : MG_ERR_BADFMT, err);
+int mg_open(const char* path, int k, int device, mg_index** out) {
+  if (!path || !out) return set_error(MG_ERR_INVAL, "null argument");
+  *out = nullptr;
+  auto t0 = std::chrono::steady_clock::now();
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
+  if (!f) return set_error(MG_ERR_IO, std::string("cannot open ") + path);
+  const uint64_t len = (uint64_t)f.tellg();
+  f.seekg(0);
+  std::vector<uint8_t> buf;
+  try {
+    buf.resize(len);
+  } catch (...) {
+    return set_error(MG_ERR_OOM, "host memory for the hashmap file");
   }
-  ix->info.n_postings = ix->host.postings.size();
-  ix->info.ref_bases = ix->host.bases.size();
-  rc = open_common(ix, k, device);
+  if (!f.read((char*)buf.data(), (std::streamsize)len)) return set_error(MG_ERR_IO, std::string("read error on ") + path);
+  mg_index* ix = new mg_index();
+  ix->info.load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  const int rc = open_image(ix, buf.data(), len, k, device);
   if (rc) {
     mg_close(ix);
     return rc;
@@ -801,26 +966,17 @@ static int open_from(mg_index* ix, int rc, const std::string& err, int k, int de
   return MG_OK;
 }
 
-int mg_open(const char* path, int k, int device, mg_index** out) {
-  if (!path || !out) return set_error(MG_ERR_INVAL, "null argument");
-  *out = nullptr;
-  mg_index* ix = new mg_index();
-  std::string err;
-  auto t0 = std::chrono::steady_clock::now();
-  int rc = mhm_load(path, k, (int)std::max(1u, std::thread::hardware_concurrency()), &ix->host, &err);
-  ix->info.load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  return open_from(ix, rc, err, k, device, out);
-}
-
 int mg_open_image(const uint8_t* image, uint64_t len, int k, int device, mg_index** out) {
   if (!image || !out) return set_error(MG_ERR_INVAL, "null argument");
   *out = nullptr;
   mg_index* ix = new mg_index();
-  std::string err;
-  auto t0 = std::chrono::steady_clock::now();
-  int rc = mhm_parse(image, len, k, (int)std::max(1u, std::thread::hardware_concurrency()), &ix->host, &err);
-  ix->info.load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  return open_from(ix, rc, err, k, device, out);
+  const int rc = open_image(ix, image, len, k, device);
+  if (rc) {
+    mg_close(ix);
+    return rc;
+  }
+  *out = ix;
+  return MG_OK;
 }
 
 void mg_close(mg_index* ix) {

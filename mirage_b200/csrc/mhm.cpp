@@ -54,19 +54,23 @@ static void parallel_for(uint64_t n, int nthreads, F f) {
 //   [w_off, w_id, w_pos, w_num] refIDMin (w_off) refPOSMin (w_off) numIDs (w_num)
 //   numIDs x (refID - refIDMin) (w_id)   w_rep (1)   numRep (w_pos)
 //   numRep x (count (w_rep), pos - refPOSMin (w_pos))
-// Returns the number of postings, or -1 when the record is malformed.
+// Returns the number of postings, or -1 when the record is malformed. Every width the writer
+// emits is at least one byte, so a record cannot hold more postings than it has bytes left; the
+// bound also keeps the sum of the counts from overflowing.
 static int64_t record_count(const uint8_t* p, const uint8_t* end) {
   if (p + 4 > end) return -1;
   int wo = p[0], wnum = p[3];
-  if (p + 4 + 2 * wo + wnum > end || wnum > 8) return -1;
-  return (int64_t)rd(p + 4 + 2 * wo, wnum);
+  if (p + 4 + 2 * wo + wnum > end || wnum > 8 || wnum < 1) return -1;
+  const uint64_t c = rd(p + 4 + 2 * wo, wnum);
+  if (c > (uint64_t)(end - p) || c > 0xFFFFFFFFull) return -1;
+  return (int64_t)c;
 }
 
 static bool decode_record(const uint8_t* p, const uint8_t* end, int word, uint32_t n_refs,
                           Posting* out, uint64_t num) {
   const uint64_t M = wmask(word);
   int wo = p[0], wid = p[1], wpos = p[2], wnum = p[3];
-  if (wo > word || wid > word || wpos > word) return false;
+  if (wo > word || wid > word || wpos > word || wo < 1 || wid < 1 || wpos < 1) return false;
   p += 4;
   uint64_t id_min = rd(p, wo), pos_min = rd(p + wo, wo);
   p += 2 * wo + wnum;
@@ -80,7 +84,7 @@ static bool decode_record(const uint8_t* p, const uint8_t* end, int word, uint32
   int wrep = p[0];
   uint64_t nrep = rd(p + 1, wpos);
   p += 1 + wpos;
-  if (wrep > word || p + nrep * (uint64_t)(wrep + wpos) > end) return false;
+  if (wrep > word || wrep < 1 || nrep > num || p + nrep * (uint64_t)(wrep + wpos) > end) return false;
   uint64_t filled = 0;
   for (uint64_t r = 0; r < nrep; r++) {
     uint64_t c = rd(p, wrep);
@@ -94,7 +98,8 @@ static bool decode_record(const uint8_t* p, const uint8_t* end, int word, uint32
   return filled == num;
 }
 
-int mhm_parse(const uint8_t* b, uint64_t L, int k, int nthreads, MhmIndex* ix, std::string* err) {
+int mhm_parse_meta(const uint8_t* b, uint64_t L, int k, MhmIndex* ix, MhmMeta* meta, bool copy_bases,
+                   std::string* err) {
   auto fail = [&](int code, const char* msg) {
     if (err) *err = msg;
     return code;
@@ -121,15 +126,8 @@ int mhm_parse(const uint8_t* b, uint64_t L, int k, int nthreads, MhmIndex* ix, s
   const uint64_t W = (uint64_t)word;
   if (n > (L - o) / (2 * W)) return fail(MHM_ERR_FORMAT, "truncated TOC");
   if (n > 0xFFFFFFFFull) return fail(MHM_ERR_LIMIT, "too many hashes");
-  ix->toc_hash.resize(n);
-  std::vector<uint64_t> sp(n);
-  for (uint64_t i = 0; i < n; i++) {
-    uint64_t h = rd(b + o, word);
-    if (h > 0x0FFFFFFFull) return fail(MHM_ERR_FORMAT, "hash wider than 28 bits");
-    ix->toc_hash[i] = (uint32_t)h;
-    sp[i] = rd(b + o + W, word);
-    o += 2 * W;
-  }
+  meta->toc_at = o;
+  o += n * 2 * W;
   // TaxIDs
   if (o + W > L) return fail(MHM_ERR_FORMAT, "truncated TaxIDs");
   uint64_t ntax = rd(b + o, word);
@@ -160,6 +158,7 @@ int mhm_parse(const uint8_t* b, uint64_t L, int k, int nthreads, MhmIndex* ix, s
   ix->n_refs = (uint32_t)nseq;
   ix->ref_len.resize(nseq);
   ix->ref_off.resize(nseq);
+  meta->bases_at = meta->bases_len = 0;
   if (nseq) {
     uint64_t first = spos[0];
     uint64_t last_end = spos[nseq - 1] + ssz[nseq - 1];
@@ -170,7 +169,9 @@ int mhm_parse(const uint8_t* b, uint64_t L, int k, int nthreads, MhmIndex* ix, s
       ix->ref_len[r] = (uint32_t)ssz[r];
       ix->ref_off[r] = spos[r] - first;
     }
-    ix->bases.assign(b + first, b + last_end);
+    meta->bases_at = first;
+    meta->bases_len = last_end - first;
+    if (copy_bases) ix->bases.assign(b + first, b + last_end);
   }
   ix->headers.resize(nhdr);
   for (uint64_t r = 0; r < nhdr; r++) {
@@ -178,6 +179,30 @@ int mhm_parse(const uint8_t* b, uint64_t L, int k, int nthreads, MhmIndex* ix, s
     uint64_t len = hsz[r];
     if (len && b[hpos[r] + len - 1] == 0) len--;
     ix->headers[r].assign((const char*)b + hpos[r], len);
+  }
+  return MHM_OK;
+}
+
+int mhm_parse(const uint8_t* b, uint64_t L, int k, int nthreads, MhmIndex* ix, std::string* err) {
+  auto fail = [&](int code, const char* msg) {
+    if (err) *err = msg;
+    return code;
+  };
+  MhmMeta meta;
+  int rc = mhm_parse_meta(b, L, k, ix, &meta, true, err);
+  if (rc) return rc;
+  const uint64_t n = ix->n_hash;
+  const int word = ix->word;
+  const uint64_t W = (uint64_t)word;
+  ix->toc_hash.resize(n);
+  std::vector<uint64_t> sp(n);
+  for (uint64_t i = 0, o = meta.toc_at; i < n; i++, o += 2 * W) {
+    uint64_t h = rd(b + o, word);
+    if (h > 0x0FFFFFFFull) return fail(MHM_ERR_FORMAT, "hash wider than 28 bits");
+    // the device directory needs the TOC ascending, as the builder writes it
+    if (i && h <= ix->toc_hash[i - 1]) return fail(MHM_ERR_FORMAT, "TOC hashes not strictly ascending");
+    ix->toc_hash[i] = (uint32_t)h;
+    sp[i] = rd(b + o + W, word);
   }
   // posting records: BufferSize = next stream position - this one; the value computed for the
   // last TOC entry is written one past the array (Hashmap.cpp:552-553), so the last hash is

@@ -49,6 +49,19 @@ enum : int {
   MHM_ERR_LIMIT = -4,
 };
 
+// Where the parts of a .mhm image lie (byte offsets into the image).
+struct MhmMeta {
+  uint64_t toc_at = 0;     // bucket TOC: n_hash x (hash, record stream position), word bytes each
+  uint64_t bases_at = 0;   // reference sequence block
+  uint64_t bases_len = 0;
+};
+
+// Everything but the bucket TOC and the posting records: header, TaxIDs, reference lengths and
+// offsets, headers, and (copy_bases) the sequence block into out->bases. toc_hash, bucket and
+// postings stay empty.
+int mhm_parse_meta(const uint8_t* data, uint64_t len, int k, MhmIndex* out, MhmMeta* meta, bool copy_bases,
+                   std::string* err);
+
 // Parse an in-memory .mhm image. nthreads host threads decode the posting records.
 int mhm_parse(const uint8_t* data, uint64_t len, int k, int nthreads, MhmIndex* out, std::string* err);
 int mhm_load(const std::string& path, int k, int nthreads, MhmIndex* out, std::string* err);

@@ -60,3 +60,45 @@ def test_device_build_large(word):
     refs, _, _ = synth.workload("uneven_fast", 0.05, seed=2024, n_reads=10)
     _same(M.build_image(refs.data, refs.offs, refs.headers, k=31, word=word, device=0),
           M.build_image(refs.data, refs.offs, refs.headers, k=31, word=word))
+
+
+MAGIC_LEN = 73  # the .mhm magic text; the bucket TOC starts 24 bytes after it
+
+
+def _toc_entry(img, i, W=4):
+    at = MAGIC_LEN + 24 + 2 * W * i
+    return at, int.from_bytes(img[at:at + W].tobytes(), "little"), int.from_bytes(img[at + W:at + 2 * W].tobytes(), "little")
+
+
+def test_device_open_matches_host_parse(golden):
+    for case in ("plain", "plain64"):
+        g = golden(case)
+        ix = M.Index(g.image)
+        host = M.inspect_image(g.image)
+        info = ix.info()
+        for f in ("n_hashes", "n_postings", "n_refs", "ref_bases", "word"):
+            assert info[f] == host[f], f
+
+
+def test_device_open_rejects_malformed(golden):
+    """Malformed images fail to open with MG_ERR_BADFMT, on the device as on the host."""
+    img = golden("plain").image
+    assert int(img[MAGIC_LEN + 12]) == 4
+    _, _, sp0 = _toc_entry(img, 0)
+    bad = []
+    bad.append(img[: len(img) * 9 // 10])                        # truncated posting area
+    b = img.copy(); b[sp0 + 1] = 0; bad.append(b)                # a zero-width refID field
+    b = img.copy(); b[sp0 + 3] = 4                               # a 4-byte count of 2^32-1 postings
+    wo = int(img[sp0])
+    b[sp0 + 4 + 2 * wo:sp0 + 8 + 2 * wo] = 0xFF; bad.append(b)
+    at0, _, _ = _toc_entry(img, 0)
+    b = img.copy(); b[at0:at0 + 4] = 0xFF; bad.append(b)         # a hash wider than 28 bits
+    at1, h1, _ = _toc_entry(img, 1)
+    b = img.copy(); b[at0:at0 + 4] = np.frombuffer((h1 + 1).to_bytes(4, "little"), np.uint8); bad.append(b)  # TOC order
+    for i, x in enumerate(bad):
+        with pytest.raises(M.MirageError) as e:
+            M.Index(x)
+        assert e.value.code == -2, i
+        with pytest.raises(M.MirageError) as e:
+            M.inspect_image(x)
+        assert e.value.code == -2, i
