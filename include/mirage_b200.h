@@ -44,6 +44,17 @@ extern "C" {
 typedef struct mg_index mg_index;
 typedef struct mg_server mg_server;
 
+/* Sequences parsed from a FASTA text (mg_parse_fasta_device). Sequence i is
+ * bases[offsets[i] .. offsets[i+1]); its header line is text[header_at[i] .. + header_len[i])
+ * of the caller's text (starting with '>', without a trailing '\r'). Free with mg_seqs_free. */
+typedef struct {
+  uint64_t n_seqs;
+  uint64_t* offsets;      /* n_seqs + 1 */
+  uint8_t* bases;
+  uint64_t* header_at;    /* n_seqs */
+  uint32_t* header_len;   /* n_seqs */
+} mg_seqs;
+
 /* A batch of reads as CSR: read i is bases[offsets[i] .. offsets[i+1]), raw sequence bytes
  * as they appear in the FASTA/FASTQ file (the library applies the reference's normalisation:
  * bytes 97..127 lose 32, Sequences.cpp:43-55, and builds the reverse complement of every read,
@@ -138,6 +149,15 @@ int mg_build_image(const uint8_t* bases, const uint64_t* offsets, uint32_t n_ref
                    const char* const* names, const int32_t* taxids, int k, int word,
                    uint8_t** image, uint64_t* len);
 void mg_free(void* p);
+
+/* Replaces Sequences::LoadInputFiles' FASTA read (GetNumberOfHeaders, TReadFastaSequencesFromMem,
+ * SequenceToUpperCase; Sequences.cpp:283-320, 57-214, 43-55) for a query or reference file held in
+ * memory, parsed by kernels on `device`: the text must start with '>'; each '>' line starts a
+ * sequence; other lines are appended without a trailing '\r'; uppercase != 0 uppercases the
+ * bases as the reference does. A line starting with '@' is refused (MG_ERR_BADINPUT): the
+ * reference reads FASTA only. */
+int mg_parse_fasta_device(int device, const uint8_t* text, uint64_t len, int uppercase, mg_seqs* out);
+void mg_seqs_free(mg_seqs* seqs);
 
 /* mg_build_image on `device`: the same image, byte for byte, built by GPU kernels (window
  * hashing, one radix sort by (hash, position), bucket sizing and record encoding; the host lays

@@ -25,7 +25,7 @@ ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LI
 
 EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
            "mg_set_timing", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
-           "mg_build_image", "mg_build_image_device", "mg_free",
+           "mg_build_image", "mg_build_image_device", "mg_parse_fasta_device", "mg_seqs_free", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_poll",
            "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error", "mg_logs_open", "mg_logs_write",
@@ -40,6 +40,11 @@ class MirageError(RuntimeError):
 
 class _Batch(C.Structure):
     _fields_ = [("n_reads", C.c_uint64), ("offsets", C.c_void_p), ("bases", C.c_void_p)]
+
+
+class _Seqs(C.Structure):
+    _fields_ = [("n_seqs", C.c_uint64), ("offsets", C.POINTER(C.c_uint64)), ("bases", C.POINTER(C.c_uint8)),
+                ("header_at", C.POINTER(C.c_uint64)), ("header_len", C.POINTER(C.c_uint32))]
 
 
 class _Result(C.Structure):
@@ -76,6 +81,9 @@ def lib() -> C.CDLL:
                                      C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(u64)]
         L.mg_build_image_device.argtypes = [i32, vp, vp, C.c_uint32, C.POINTER(C.c_char_p), vp, i32, i32,
                                             C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(u64)]
+        L.mg_parse_fasta_device.argtypes = [i32, vp, u64, i32, C.POINTER(_Seqs)]
+        L.mg_seqs_free.argtypes = [C.POINTER(_Seqs)]
+        L.mg_seqs_free.restype = None
         L.mg_free.argtypes = [vp]
         L.mg_free.restype = None
         L.mg_score_batch.argtypes = [vp, C.POINTER(_Batch), C.POINTER(_Result)]
@@ -129,6 +137,29 @@ def gather_bandwidth(device: int = 0, buffer_bytes: int = 1 << 30) -> float:
     out = C.c_double()
     _check(lib().mg_gather_bandwidth(device, buffer_bytes, C.byref(out)), "mg_gather_bandwidth")
     return out.value
+
+
+def parse_fasta(text, device: int = 0, uppercase: bool = True):
+    """Parse a FASTA text on `device` as the reference's loader does; returns (bases, offsets,
+    headers) with the bases and offsets as numpy arrays and the header lines as bytes."""
+    t = _u8(np.frombuffer(text, np.uint8) if isinstance(text, (bytes, bytearray)) else text)
+    s = _Seqs()
+    _check(lib().mg_parse_fasta_device(device, t.ctypes.data, len(t), 1 if uppercase else 0, C.byref(s)),
+           "mg_parse_fasta_device")
+    try:
+        n = int(s.n_seqs)
+        offs = np.ctypeslib.as_array(s.offsets, shape=(n + 1,)).copy()
+        total = int(offs[-1])
+        bases = np.ctypeslib.as_array(s.bases, shape=(total,)).copy() if total else np.zeros(0, np.uint8)
+        heads = []
+        if n:
+            at = np.ctypeslib.as_array(s.header_at, shape=(n,))
+            ln = np.ctypeslib.as_array(s.header_len, shape=(n,))
+            tb = t.tobytes()
+            heads = [tb[int(a):int(a) + int(b)] for a, b in zip(at, ln)]
+        return bases, offs, heads
+    finally:
+        lib().mg_seqs_free(C.byref(s))
 
 
 def build_image(bases, offsets, names, k: int = 31, word: int = 0, taxids=None, device: int | None = None) -> np.ndarray:

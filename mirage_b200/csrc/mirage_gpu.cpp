@@ -84,37 +84,29 @@ struct Seqs {
   std::vector<std::string> headers;  // header line with '>' / '@'
 };
 
-// FASTA / FASTQ as the reference reads them (Sequences.cpp:57-214): a line starting with '>'
-// or '@' opens a record; in FASTQ only the first line after the header is sequence; '\r'
-// line ends are dropped.
-bool read_fasta(const std::string& path, Seqs* out, bool uppercase) {
-  std::ifstream f(path, std::ios::binary);
+// A FASTA file as the reference's loader reads it (Sequences.cpp:283-320, 57-214), parsed on the
+// GPU (mg_parse_fasta_device); uppercase as the loader does for references. Returns false when the
+// file cannot be read; a file the reference would not load either (not starting with '>', or
+// FASTQ) stops the program with the library's message.
+bool read_fasta(const std::string& path, int gpu, Seqs* out, bool uppercase) {
+  std::ifstream f(path, std::ios::binary | std::ios::ate);
   if (!f) return false;
-  std::string line;
-  bool fastq = false;
-  int qline = 0;
-  bool open = false;
-  while (std::getline(f, line)) {
-    if (!line.empty() && line.back() == '\r') line.pop_back();
-    if (!line.empty() && (line[0] == '>' || line[0] == '@') && !(fastq && qline > 0)) {
-      if (open) out->offs.push_back(out->bases.size());
-      out->headers.push_back(line);
-      fastq = line[0] == '@';
-      qline = 0;
-      open = true;
-      continue;
-    }
-    if (!open) continue;
-    if (fastq) {
-      if (qline++ != 0) continue;
-    }
-    for (char ch : line) {
-      uint8_t c = (uint8_t)ch;
-      if (uppercase && (int8_t)c > 96) c -= 32;  // Sequences.cpp:43-55
-      out->bases.push_back(c);
-    }
+  const uint64_t len = (uint64_t)f.tellg();
+  f.seekg(0);
+  std::vector<uint8_t> text(len);
+  if (len && !f.read((char*)text.data(), (std::streamsize)len)) return false;
+  mg_seqs s{};
+  const int rc = mg_parse_fasta_device(gpu, text.data(), len, uppercase ? 1 : 0, &s);
+  if (rc) {
+    std::fprintf(stderr, "mirage_gpu: reading %s failed: %s (%s)\n", path.c_str(), mg_strerror(rc), mg_last_error());
+    std::exit(1);
   }
-  if (open) out->offs.push_back(out->bases.size());
+  out->offs.assign(s.offsets, s.offsets + s.n_seqs + 1);
+  out->bases.assign(s.bases, s.bases + s.offsets[s.n_seqs]);
+  out->headers.resize(s.n_seqs);
+  for (uint64_t i = 0; i < s.n_seqs; i++)
+    out->headers[i].assign((const char*)text.data() + s.header_at[i], s.header_len[i]);
+  mg_seqs_free(&s);
   return true;
 }
 
@@ -202,7 +194,7 @@ int main(int argc, char** argv) {
     if (rc) die("loading the hashmap", rc);
   } else {
     Seqs refs;
-    if (!read_fasta(reference, &refs, true)) {
+    if (!read_fasta(reference, gpu, &refs, true)) {
       std::fprintf(stderr, "Could not find or read fasta file: %s\n", reference.c_str());
       return 1;
     }
@@ -235,7 +227,7 @@ int main(int argc, char** argv) {
   for (uint32_t r = 0; r < info.n_refs; r++) mg_index_reference(ix, r, &ref_headers[r], &taxids[r], nullptr);
 
   Seqs q;
-  if (!read_fasta(query, &q, false)) {
+  if (!read_fasta(query, gpu, &q, false)) {
     std::fprintf(stderr, "Could not find or read fasta file: %s\n", query.c_str());
     return 1;
   }

@@ -119,6 +119,7 @@ struct Opts {
   int repeat = 1;
   int k = 31;
   bool first_only = true;
+  bool parse_only = false;
 };
 
 static void usage() {
@@ -147,6 +148,7 @@ int main(int argc, char** argv) {
     else if (a == "--repeat") o.repeat = std::stoi(next());
     else if (a == "--k") o.k = std::stoi(next());
     else if (a == "--all-groups") o.first_only = false;
+    else if (a == "--parse-only") o.parse_only = true;
     else usage();
   }
   if (o.mhm.empty() || o.reads.empty()) usage();
@@ -193,6 +195,29 @@ int main(int argc, char** argv) {
                                                              : analyser.ConsiderThreshold;
   auto t_load1 = std::chrono::steady_clock::now();
 
+  // --parse-only: the query file as the reference's loader parsed it (forward sequences, then
+  // the headers), one "Q <length> <hex bytes>" / "H <hex bytes>" line each
+  if (o.parse_only) {
+    FILE* f = o.out.empty() ? stdout : std::fopen(o.out.c_str(), "w");
+    const size_t nf = sequences.inputSequences->size() / 2;
+    std::fprintf(f, "N %zu %zu\n", nf, sequences.inputHeaders.size());
+    auto hex = [&](const char* p, size_t n) {
+      for (size_t i = 0; i < n; i++) std::fprintf(f, "%02x", (unsigned char)p[i]);
+    };
+    for (size_t i = 0; i < nf; i++) {
+      const std::vector<char>& q = (*sequences.inputSequences)[i];
+      std::fprintf(f, "Q %zu ", q.size());
+      hex(q.data(), q.size());
+      std::fprintf(f, "\n");
+    }
+    for (auto* h : sequences.inputHeaders) {
+      std::fprintf(f, "H ");
+      hex(h->data(), h->size());
+      std::fprintf(f, "\n");
+    }
+    if (f != stdout) std::fclose(f);
+    return 0;
+  }
   size_t n_reads = sequences.inputSequences->size() / 2;
   if (o.limit >= 0 && (size_t)o.limit < n_reads) n_reads = (size_t)o.limit;
 
