@@ -88,8 +88,10 @@ __device__ __forceinline__ uint8_t complement_dev(uint8_t c) {
 __device__ __forceinline__ float log_dev_raw(float x) { return __double2float_rn(log((double)x)); }
 
 // logf exactly as the host libm computes it, for x in [1, 2^20): the device value, replaced
-// by the host's where the two were found to differ when the index was opened.
-__device__ __forceinline__ float ref_logf(const DevIndex& ix, float x, int* err) {
+// by the host's where the two were found to differ when the index was opened. Out of line: called
+// once per scored candidate, and keeping its double-precision log out of the warp tier's hot
+// code measurably reduces instruction-fetch stalls there.
+static __device__ __noinline__ float ref_logf(const DevIndex& ix, float x, int* err) {
   uint32_t b = __float_as_uint(x);
   if (b < kLogLoBits || b >= kLogHiBits) {
     *err |= kErrLogRange;
@@ -109,7 +111,7 @@ __device__ __forceinline__ float ref_logf(const DevIndex& ix, float x, int* err)
 
 // MatrixResult::GetRelativeScore (MatrixResult.cpp:21-29) with explicit IEEE roundings:
 // lenMax float; scoreMax in double then float; score + 1 in float; logf / logf in float.
-__device__ __forceinline__ float relative_score(const DevIndex& ix, float qlen, float rlen, float score, int* err) {
+static __device__ __noinline__ float relative_score(const DevIndex& ix, float qlen, float rlen, float score, int* err) {
   const float len_max = qlen < rlen ? qlen : rlen;
   const double lm = (double)len_max;
   const float score_max = __double2float_rn(__dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(lm, __dadd_rn(lm, 1.0)), 2.0), lm), 1.0));

@@ -53,9 +53,16 @@ int ensure_workspace(Workspace& ws, uint64_t n_reads, uint64_t n_bases, bool hos
 // chain (optional, device, 16 bytes): for one chunk of a larger batch, [0] the candidates of the
 // earlier chunks (output offsets continue from there and the count is advanced), [8] the batch's
 // error bits (accumulated instead of the per-call counter).
+// For chunks on two streams: the scan waits for the previous chunk's (wait_prev), then the
+// running total is copied to *snap (pinned host memory) and `scanned` is recorded.
+struct ChainSync {
+  cudaEvent_t wait_prev = nullptr;
+  cudaEvent_t scanned = nullptr;
+  unsigned long long* snap = nullptr;
+};
 int run_pipeline(mg_index* ix, Workspace& ws, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                  mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain,
-                 unsigned long long* chain = nullptr);
+                 unsigned long long* chain = nullptr, const ChainSync* cs = nullptr);
 // Wait for st, read the error word and the candidate count of the call that used ws.
 int finish_errors(Workspace& ws, cudaStream_t st, uint64_t* n_cands);
 // The pipeline's counters after the stream drains.
@@ -85,8 +92,10 @@ struct mg_index {
   cudaStream_t stream = nullptr;
   // chunked batched form: copy streams and per-chunk events (made on first use)
   static constexpr int kMaxChunks = 8;
-  cudaStream_t h2d = nullptr, d2h = nullptr;
-  cudaEvent_t ev_in[kMaxChunks], ev_done[kMaxChunks];
+  cudaStream_t h2d = nullptr, d2h = nullptr, stream2 = nullptr;  // stream2: odd chunks
+  cudaEvent_t ev_in[kMaxChunks], ev_done[kMaxChunks], ev_scan[kMaxChunks];
+  unsigned long long* h_snap = nullptr;  // pinned: running candidate totals after each chunk
+  mg::Workspace ws2;                     // scratch of the odd chunks
   bool chunk_made = false;
   std::mutex mu;
   mg_index_info info{};

@@ -694,7 +694,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 // 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
-                        bool plain, unsigned long long* chain) {
+                        bool plain, unsigned long long* chain, const ChainSync* cs) {
   uint8_t* ctr = w.ctr.as<uint8_t>();
   CU(cudaMemsetAsync(ctr, 0, 256, st));
   BatchDev b;
@@ -762,7 +762,10 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
     const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
     unsigned long long* sums = w.sums.as<unsigned long long>();
     k_count_sums<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums);
+    if (cs && cs->wait_prev) CU(cudaStreamWaitEvent(st, cs->wait_prev, 0));
     k_scan_sums<<<1, kScanBlock, 0, st>>>(sums, nb, (unsigned long long*)(ctr + 40), chain);
+    if (cs && cs->snap) CU(cudaMemcpyAsync(cs->snap, chain, 8, cudaMemcpyDeviceToHost, st));
+    if (cs && cs->scanned) CU(cudaEventRecord(cs->scanned, st));
     k_scatter<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums, sd, d_out, cap, b.err);
     if (tm) CU(cudaEventRecord(ix->ev[5], st));
     CU(cudaGetLastError());
@@ -827,51 +830,70 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   if (!ix->chunk_made) {
     CU(cudaStreamCreateWithFlags(&ix->h2d, cudaStreamNonBlocking));
     CU(cudaStreamCreateWithFlags(&ix->d2h, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&ix->stream2, cudaStreamNonBlocking));
     for (int i = 0; i < mg_index::kMaxChunks; i++) {
       CU(cudaEventCreateWithFlags(&ix->ev_in[i], cudaEventDisableTiming));
       CU(cudaEventCreateWithFlags(&ix->ev_done[i], cudaEventDisableTiming));
+      CU(cudaEventCreateWithFlags(&ix->ev_scan[i], cudaEventDisableTiming));
     }
+    CU(cudaMallocHost((void**)&ix->h_snap, mg_index::kMaxChunks * 8));
     ix->chunk_made = true;
   }
   if (w.chain.alloc(16)) return set_error(MG_ERR_OOM, "chunk counters");
-  cudaStream_t st = ix->stream;
   const int nc = (int)std::min<uint64_t>(mg_index::kMaxChunks, n / kChunkReads);
+  // the odd chunks run on a second stream with their own scratch, so that one chunk's tail
+  // overlaps the next chunk's start; the compaction scans stay in chunk order
+  const uint64_t max_chunk = (n + nc - 1) / nc + 1;
+  int rc = ensure_workspace(ix->ws2, max_chunk, 0, false);
+  if (rc) return rc;
+  cudaStream_t cst[2] = {ix->stream, ix->stream2};
+  Workspace* cws[2] = {&w, &ix->ws2};
   unsigned long long* chain = w.chain.as<unsigned long long>();
-  CU(cudaMemsetAsync(chain, 0, 16, st));
+  CU(cudaMemsetAsync(chain, 0, 16, ix->h2d));
   CU(cudaMemcpyAsync(w.offs.p, batch->offsets, (n + 1) * 8, cudaMemcpyHostToDevice, ix->h2d));
-  int rc = MG_OK;
   for (int i = 0; i < nc && rc == MG_OK; i++) {
     const uint64_t r0 = n * i / nc, r1 = n * (i + 1) / nc;
     const uint64_t b0 = batch->offsets[r0], b1 = batch->offsets[r1];
+    cudaStream_t st = cst[i & 1];
     if (b1 > b0)
       CU(cudaMemcpyAsync(w.bases.as<uint8_t>() + b0, batch->bases + b0, b1 - b0, cudaMemcpyHostToDevice, ix->h2d));
     CU(cudaEventRecord(ix->ev_in[i], ix->h2d));
     CU(cudaStreamWaitEvent(st, ix->ev_in[i], 0));
-    rc = run_pipeline(ix, w, r1 - r0, w.offs.as<uint64_t>() + r0, w.bases.as<uint8_t>(),
-                      w.reads.as<mg_read_result>() + r0, w.cands.as<mg_candidate>(), out->cand_cap, st, false, chain);
+    const ChainSync cs{i ? ix->ev_scan[i - 1] : nullptr, ix->ev_scan[i], ix->h_snap + i};
+    rc = run_pipeline(ix, *cws[i & 1], r1 - r0, w.offs.as<uint64_t>() + r0, w.bases.as<uint8_t>(),
+                      w.reads.as<mg_read_result>() + r0, w.cands.as<mg_candidate>(), out->cand_cap, st, false, chain,
+                      &cs);
     if (rc) break;
     CU(cudaEventRecord(ix->ev_done[i], st));
+  }
+  // results back in chunk order as each chunk completes: its reads, then its candidates (whose
+  // range the running total snapshot gives)
+  uint64_t lo = 0;
+  for (int i = 0; i < nc && rc == MG_OK; i++) {
+    const uint64_t r0 = n * i / nc, r1 = n * (i + 1) / nc;
+    CU(cudaEventSynchronize(ix->ev_scan[i]));
+    const uint64_t hi = ix->h_snap[i];
     CU(cudaStreamWaitEvent(ix->d2h, ix->ev_done[i], 0));
     CU(cudaMemcpyAsync(out->reads + r0, w.reads.as<mg_read_result>() + r0, (r1 - r0) * sizeof(mg_read_result),
                        cudaMemcpyDeviceToHost, ix->d2h));
+    const uint64_t a = std::min(lo, out->cand_cap), b = std::min(hi, out->cand_cap);
+    if (b > a)
+      CU(cudaMemcpyAsync(out->cands + a, w.cands.as<mg_candidate>() + a, (b - a) * sizeof(mg_candidate),
+                         cudaMemcpyDeviceToHost, ix->d2h));
+    lo = hi;
   }
   unsigned long long h[2] = {0, 0};
-  if (rc == MG_OK) CU(cudaMemcpyAsync(h, chain, 16, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(ix->h2d));
-  CU(cudaStreamSynchronize(st));
+  CU(cudaStreamSynchronize(ix->stream));
+  CU(cudaStreamSynchronize(ix->stream2));
+  if (rc == MG_OK) CU(cudaMemcpy(h, chain, 16, cudaMemcpyDeviceToHost));
   CU(cudaStreamSynchronize(ix->d2h));
   if (rc) return rc;
   int err = 0;
   std::memcpy(&err, &h[1], 4);
   out->n_cands = h[0];
   if (err & kErrArena) return kRunWhole;
-  rc = error_status(err);
-  if (rc) return rc;
-  if (h[0]) {
-    CU(cudaMemcpyAsync(out->cands, w.cands.p, h[0] * sizeof(mg_candidate), cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
-  }
-  return MG_OK;
+  return error_status(err);
 }
 
 static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bool plain) {
@@ -989,13 +1011,17 @@ void mg_close(mg_index* ix) {
   if (ix->stream) cudaStreamDestroy(ix->stream);
   if (ix->events_made)
     for (auto& e : ix->ev) cudaEventDestroy(e);
+  ix->ws2.release();
   if (ix->chunk_made) {
     cudaStreamDestroy(ix->h2d);
     cudaStreamDestroy(ix->d2h);
+    cudaStreamDestroy(ix->stream2);
     for (int i = 0; i < mg_index::kMaxChunks; i++) {
       cudaEventDestroy(ix->ev_in[i]);
       cudaEventDestroy(ix->ev_done[i]);
+      cudaEventDestroy(ix->ev_scan[i]);
     }
+    cudaFreeHost(ix->h_snap);
   }
   delete ix;
 }
