@@ -64,6 +64,11 @@ struct BatchDev {
 
 __device__ __forceinline__ uint32_t hash28_dev(const uint8_t* p, int len) {
   uint32_t h = 2166136261u;
+  if (len == 17) {  // the window of the default k (31), unrolled
+#pragma unroll
+    for (int i = 0; i < 17; i++) h = (h * 16777619u) ^ p[i];
+    return ((h >> 28) ^ h) & 0x0FFFFFFFu;
+  }
   for (int i = 0; i < len; i++) h = (h * 16777619u) ^ p[i];
   return ((h >> 28) ^ h) & 0x0FFFFFFFu;
 }

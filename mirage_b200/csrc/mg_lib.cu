@@ -819,7 +819,7 @@ int error_status(int err) {
 constexpr uint64_t kChunkReads = 131072;
 constexpr int kRunWhole = 1;
 
-// Batched form with host buffers, in chunks: chunk i's bases are copied on the index's h2d stream
+// Batched form with host buffers, in chunks: chunk i's offsets and bases are copied on the index's h2d stream
 // while chunk i-1 is classified on its compute stream, and chunk i's read results go back on the
 // d2h stream while chunk i+1 is classified. The chunks share the device output: the compaction
 // continues the candidate offsets of the earlier chunks (run_pipeline's chain), so cand_off is an
@@ -841,20 +841,37 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   }
   if (w.chain.alloc(16)) return set_error(MG_ERR_OOM, "chunk counters");
   const int nc = (int)std::min<uint64_t>(mg_index::kMaxChunks, n / kChunkReads);
+  // chunk boundaries, weighted so that the first chunk (whose upload nothing hides) and the last
+  // (whose classification and copy back nothing hides) are the smallest
+  static const int kWeight[mg_index::kMaxChunks] = {1, 2, 3, 3, 3, 3, 2, 1};
+  uint64_t bound[mg_index::kMaxChunks + 1];
+  {
+    const bool weighted = nc == mg_index::kMaxChunks;
+    uint64_t wsum = 0, acc = 0;
+    for (int i = 0; i < nc; i++) wsum += weighted ? kWeight[i] : 1;
+    bound[0] = 0;
+    for (int i = 0; i < nc; i++) {
+      acc += weighted ? kWeight[i] : 1;
+      bound[i + 1] = n * acc / wsum;
+    }
+  }
+  uint64_t max_chunk = 0;
+  for (int i = 0; i < nc; i++) max_chunk = std::max(max_chunk, bound[i + 1] - bound[i]);
   // the odd chunks run on a second stream with their own scratch, so that one chunk's tail
   // overlaps the next chunk's start; the compaction scans stay in chunk order
-  const uint64_t max_chunk = (n + nc - 1) / nc + 1;
-  int rc = ensure_workspace(ix->ws2, max_chunk, 0, false);
+  int rc = ensure_workspace(ix->ws2, max_chunk + 1, 0, false);
   if (rc) return rc;
   cudaStream_t cst[2] = {ix->stream, ix->stream2};
   Workspace* cws[2] = {&w, &ix->ws2};
   unsigned long long* chain = w.chain.as<unsigned long long>();
   CU(cudaMemsetAsync(chain, 0, 16, ix->h2d));
-  CU(cudaMemcpyAsync(w.offs.p, batch->offsets, (n + 1) * 8, cudaMemcpyHostToDevice, ix->h2d));
   for (int i = 0; i < nc && rc == MG_OK; i++) {
-    const uint64_t r0 = n * i / nc, r1 = n * (i + 1) / nc;
+    const uint64_t r0 = bound[i], r1 = bound[i + 1];
     const uint64_t b0 = batch->offsets[r0], b1 = batch->offsets[r1];
     cudaStream_t st = cst[i & 1];
+    // each chunk's offsets travel with its bases (the shared boundary entry twice, same value)
+    CU(cudaMemcpyAsync(w.offs.as<uint64_t>() + r0, batch->offsets + r0, (r1 - r0 + 1) * 8, cudaMemcpyHostToDevice,
+                       ix->h2d));
     if (b1 > b0)
       CU(cudaMemcpyAsync(w.bases.as<uint8_t>() + b0, batch->bases + b0, b1 - b0, cudaMemcpyHostToDevice, ix->h2d));
     CU(cudaEventRecord(ix->ev_in[i], ix->h2d));
@@ -870,7 +887,7 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   // range the running total snapshot gives)
   uint64_t lo = 0;
   for (int i = 0; i < nc && rc == MG_OK; i++) {
-    const uint64_t r0 = n * i / nc, r1 = n * (i + 1) / nc;
+    const uint64_t r0 = bound[i], r1 = bound[i + 1];
     CU(cudaEventSynchronize(ix->ev_scan[i]));
     const uint64_t hi = ix->h_snap[i];
     CU(cudaStreamWaitEvent(ix->d2h, ix->ev_done[i], 0));
