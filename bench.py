@@ -48,6 +48,9 @@ N_READS = 1_000_000
 # kernels one batched call launches: dual-strand warp tier, general warp tier, block tier,
 # global tier, candidate count, scan, scatter
 LAUNCHES_PER_BATCH = 7
+# DRAM bytes (read + write) of one k_classify_dual launch on the default workload (1,000,000
+# reads, scale 1.0), from one ncu capture: profiles/dram_k_classify_dual_uneven-full_1M-reads.md
+DUAL_TRAFFIC_DEFAULT = 5_633_708_800 + 83_831_808
 
 
 def log(*a):
@@ -465,8 +468,12 @@ def main():
         warp_ms = (kernel_ms[0] + kernel_ms[1]) / args.steps
         achieved = ab["bytes"] / (warp_ms / 1000) / 1e9
         gather = M.gather_bandwidth(local, 4 << 30)
+        default_run = args.scale == 1.0 and args.reads == N_READS
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm or 6650.0, "unit": "GB/s",
-                "frac": achieved / (hbm or 6650.0), "traffic": None,
+                "frac": achieved / (hbm or 6650.0),
+                "traffic": DUAL_TRAFFIC_DEFAULT if default_run else None,
+                "traffic_what": "DRAM bytes per k_classify_dual launch, one ncu capture of this workload "
+                                "(profiles/dram_k_classify_dual_uneven-full_1M-reads.md)" if default_run else None,
                 "gather_peak": gather, "frac_of_gather": achieved / gather,
                 "gather_peak_what": "random 32-byte sector gathers, 8 lanes per sector, over a 4 GiB buffer "
                                     "(mg_gather_bandwidth), measured in this run",
