@@ -44,7 +44,9 @@ int set_error(int code, const std::string& msg) {
 
 // ------------------------------------------------------------------------------ tiers
 
-// Warp tier: one warp per read, workspace in shared memory (8 warps per block).
+// Warp tiers: one warp per read, workspace in shared memory (8 warps per block). The dual-strand
+// tier takes reads up to kLeanQ bases with at most 64 postings and 8 scored candidates per strand;
+// the general warp tier takes its leftovers within the limits below.
 constexpr int kW1Warps = 8;
 constexpr int kW1Q = 320, kW1Seeds = 20, kW1E = 128, kW1C = 8;
 constexpr int kW1Chunk = 4;  // reads taken per work-stealing step
@@ -669,10 +671,6 @@ static int open_image(mg_index* ix, const uint8_t* image, uint64_t L, int k, int
 }
 
 // ---------------------------------------------------------------------- classification
-
-struct Plan {
-  bool plain;  // block-per-read form
-};
 
 int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host_io) {
   uint64_t arena_cap = std::max<uint64_t>(1 << 16, n_reads * 2);
