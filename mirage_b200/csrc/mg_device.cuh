@@ -97,13 +97,16 @@ __device__ __forceinline__ float log_dev_raw(float x) { return __double2float_rn
 // once per scored candidate, and keeping its double-precision log out of the warp tier's hot
 // code measurably reduces instruction-fetch stalls there.
 static __device__ __noinline__ float ref_logf(const DevIndex& ix, float x, int* err) {
-  uint32_t b = __float_as_uint(x);
-  if (b < kLogLoBits || b >= kLogHiBits) {
+  const uint32_t b = __float_as_uint(x);
+  const bool in = b >= kLogLoBits && b < kLogHiBits;
+  const uint32_t r = in ? b - kLogLoBits : 0u;
+  const uint32_t word = __ldg(ix.logx_bitmap + (r >> 5));  // in flight while the logarithm runs
+  const float v = log_dev_raw(x);
+  if (!in) {
     *err |= kErrLogRange;
-    return log_dev_raw(x);
+    return v;
   }
-  uint32_t r = b - kLogLoBits;
-  if (ix.logx_bitmap[r >> 5] & (1u << (r & 31))) {
+  if (word & (1u << (r & 31))) {
     uint32_t lo = 0, hi = ix.n_logx;
     while (lo < hi) {
       uint32_t mid = (lo + hi) >> 1;
@@ -111,7 +114,7 @@ static __device__ __noinline__ float ref_logf(const DevIndex& ix, float x, int* 
     }
     return ix.logx_vals[lo];
   }
-  return log_dev_raw(x);
+  return v;
 }
 
 // MatrixResult::GetRelativeScore (MatrixResult.cpp:21-29) with explicit IEEE roundings:

@@ -31,6 +31,7 @@ struct DualSmem {
                                 // diagonal runs on: z (run ends) and segmax (reference heads)
   mg_candidate cb[2][kDualC];   // scored candidates in ascending refID
   uint8_t q[2][kLeanQ];         // strand bases: forward, reverse complement
+  uint8_t q_pad[8];             // word reads of q[1]'s last bases run up to 7 bytes past it
 };
 static_assert(sizeof(uint32_t) * 2 * 3 * kDualE >= sizeof(uint32_t) * 32 * kCovWords, "coverage bitmaps");
 
@@ -39,6 +40,27 @@ __device__ __forceinline__ unsigned long long upto64(int i) {  // bits 0..i
 }
 __device__ __forceinline__ unsigned long long below64(int i) {  // bits 0..i-1
   return i <= 0 ? 0ull : upto64(i - 1);
+}
+
+// Four bytes from p (any alignment) as one little-endian word, read as two aligned words.
+__device__ __forceinline__ uint32_t bytes4(const uint8_t* p) {
+  const uintptr_t a = (uintptr_t)p;
+  const uint32_t* w = (const uint32_t*)(a & ~(uintptr_t)3);
+  return __funnelshift_r(w[0], w[1], (uint32_t)(a & 3) * 8u);
+}
+
+// tail_walk (mg_kernels.cuh) four bytes at a time: the length of the common prefix of the query
+// from lq and the reference from lr, at most min(rlen - lr, k, L - lq). Reads up to 7 bytes past
+// the last compared byte of each side (the index's base array and the strand buffers are padded).
+__device__ __forceinline__ uint32_t tail_walk4(const uint8_t* q, const uint8_t* rs, uint32_t L, uint32_t rlen,
+                                               uint32_t lq, uint32_t lr, uint32_t k) {
+  if (lq >= L || lr >= rlen) return 0;
+  const uint32_t lim = min(min(rlen - lr, k), L - lq);
+  for (uint32_t i = 0; i < lim; i += 4) {
+    const uint32_t x = bytes4(q + lq + i) ^ bytes4(rs + lr + i);
+    if (x) return min(i + ((uint32_t)(__ffs(x) - 1) >> 3), lim);
+  }
+  return lim;
 }
 
 // Bits of a full-warp ballot that belong to this lane's half.
@@ -231,7 +253,7 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
         const uint32_t lr = s_pos[i] + step, lq = s_j[i] * step + step;
         const uint8_t* rs = ix.bases + ix.ref_off[ref];
         const uint32_t rlen = ix.ref_len[ref];
-        const uint32_t tail = tail_walk(q, rs, L, rlen, lq, lr, k);
+        const uint32_t tail = tail_walk4(q, rs, L, rlen, lq, lr, k);
         const uint32_t head = head_walk(q, rs, sq, sr, k);
         const uint32_t tot = tail + head + (lq - sq);
         if (tot >= k) zz = ((sq - head) << 16) | tot;
