@@ -66,11 +66,16 @@ __device__ __forceinline__ uint32_t tail_walk4(const uint8_t* q, const uint8_t* 
 // Bits of a full-warp ballot that belong to this lane's half.
 __device__ __forceinline__ uint32_t half_bits(uint32_t ballot, int sh) { return (ballot >> sh) & 0xFFFFu; }
 
+// A candidate before scoring: the sum of T(T+1)/2 over its scored runs, the sum of T and the
+// covered query bases, as the bits of the rel, score and pct fields.
+__device__ __forceinline__ mg_candidate raw_candidate(uint32_t ref, uint32_t sumr, uint32_t sumc, uint32_t hits) {
+  return mg_candidate{ref, __uint_as_float(sumr), __uint_as_float(sumc), __uint_as_float(hits)};
+}
+
 // Both strands of one read (bases already in S.q). Warp-uniform return: kStrandOk, or
-// kStrandOverflow when either strand does not fit. Each lane receives its half's strand results:
-// *n_out scored candidates in S.cb[half] (ascending refID) and the strand's HighestScore.
-__device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_t* n_out, float* hi_out,
-                            int* err) {
+// kStrandOverflow when either strand does not fit. Each lane receives its half's strand result:
+// *n_out candidates in S.cb[half] (ascending refID), raw (raw_candidate).
+__device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_t* n_out) {
   const unsigned FULL = 0xffffffffu;
   const uint32_t EMPTY = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15, sh = half * 16;
@@ -85,7 +90,6 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
   uint32_t* tkey = S.t[half][0];
   uint32_t* tval = S.t[half][1];
   *n_out = 0;
-  *hi_out = -1.0f;
   if (L <= k) return kStrandOk;
   const uint32_t ns = (L - k + step - 1) / step;
   if (ns > 32) return kStrandOverflow;
@@ -275,11 +279,11 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
   for (int s = 0; s < nkw; s++) Sm |= (unsigned long long)half_bits(__ballot_sync(FULL, is_cand(hl + 16 * s)), sh) << (16 * s);
   const int n_sc = __popcll(Sm);
   if (__any_sync(FULL, n_sc > kDualC)) return kStrandOverflow;
-  //    sums, coverage and scores, one lane per candidate (MatrixCPU.cpp:18-214)
+  //    sums and coverage, one lane per candidate (MatrixCPU.cpp:18-208); the scores from them are
+  //    k_finish_dual's (MatrixCPU.cpp:209-212, MatrixResult.cpp:21-29)
   const uint32_t nw = (L + 31) / 32;
   uint32_t* cov = &S.c[0][0][0] + lane * kCovWords;
   mg_candidate* cb = S.cb[half];
-  float hi = -1.0f;
   for (int s = 0; s < nkw; s++) {
     const int h = hl + 16 * s;
     if (!((Sm >> h) & 1ull)) continue;
@@ -301,18 +305,44 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
     }
     uint32_t hits = 0;
     for (uint32_t wd = 0; wd < nw; wd++) hits += __popc(cov[wd]);
-    float sc, pc;
-    final_score(sumr, sumc, hits, L, &sc, &pc);
-    const uint32_t cref = s_ref[h];
-    const float rl = relative_score_tab(ix, L, ix.ref_len[cref], sc, err);
-    cb[__popcll(Sm & below64(h))] = mg_candidate{cref, rl, sc, pc};
-    hi = fmaxf(hi, rl);
+    cb[__popcll(Sm & below64(h))] = raw_candidate(s_ref[h], sumr, sumc, hits);
   }
-  for (int o = 8; o > 0; o >>= 1) hi = fmaxf(hi, __shfl_xor_sync(FULL, hi, o));
   __syncwarp();
   *n_out = (uint32_t)n_sc;
-  *hi_out = hi;
   return kStrandOk;
+}
+
+// The dual tier's read result: the raw candidates go to the read's staging slots (or the arena
+// when there are more than kSlots) and the read is marked kReadUnscored for k_finish_dual; a read
+// without candidates is final here (what write_read_result_s gives with no candidate).
+__device__ __forceinline__ void write_read_raw(const BatchDev& b, uint32_t r, uint32_t n0, uint32_t n1,
+                                               const mg_candidate* cb0, const mg_candidate* cb1, mg_candidate* stage,
+                                               mg_candidate* arena, uint64_t arena_cap, unsigned long long* arena_n,
+                                               int* errw) {
+  const uint32_t tot = n0 + n1;
+  if (tot == 0) {
+    b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
+    return;
+  }
+  uint32_t where = 0;
+  uint8_t mark = kReadUnscored;
+  mg_candidate* dst = stage + (uint64_t)r * kSlots;
+  if (tot > (uint32_t)kSlots) {
+    const unsigned long long at = atomicAdd(arena_n, (unsigned long long)tot);
+    if (at + tot > arena_cap) {  // the call grows the arena and runs the batch again
+      atomicOr(errw, kErrArena);
+      dst = nullptr;
+      mark = 0;
+    } else {
+      dst = arena + at;
+      where = (uint32_t)at;
+    }
+  }
+  if (dst) {
+    for (uint32_t c = 0; c < n0; c++) dst[c] = cb0[c];
+    for (uint32_t c = 0; c < n1; c++) dst[n0 + c] = cb1[c];
+  }
+  b.reads[r] = mg_read_result{-1.0f, where, (uint16_t)n0, (uint16_t)n1, mark, 0, 0};
 }
 
 // Read r on the dual path; false when it does not fit (the caller hands it on).
@@ -342,14 +372,9 @@ __device__ bool process_read_dual(const DevIndex& ix, const BatchDev& b, uint32_
   }
   __syncwarp();
   uint32_t nh;
-  float hh;
-  int err = 0;
-  if (dual_strands(ix, L, S, &nh, &hh, &err) != kStrandOk) return false;
-  err = (int)__reduce_or_sync(FULL, (unsigned)err);
+  if (dual_strands(ix, L, S, &nh) != kStrandOk) return false;
   const uint32_t n0 = __shfl_sync(FULL, nh, 0), n1 = __shfl_sync(FULL, nh, 16);
-  const float h0 = __shfl_sync(FULL, hh, 0), h1 = __shfl_sync(FULL, hh, 16);
-  if (lane == 0)
-    write_read_result_s(b, r, false, n0, n1, h0, h1, S.cb[0], S.cb[1], stage, arena, arena_cap, arena_n, errw, err);
+  if (lane == 0) write_read_raw(b, r, n0, n1, S.cb[0], S.cb[1], stage, arena, arena_cap, arena_n, errw);
   __syncwarp();
   return true;
 }

@@ -20,6 +20,10 @@ namespace mg {
 // place them in an overflow arena.
 constexpr int kSlots = 4;
 
+// mg_read_result::strand of a read whose candidates hold raw sums (the dual-strand tier leaves the
+// scores to k_finish_dual); never left in a finished result.
+constexpr uint8_t kReadUnscored = 0xFD;
+
 struct Caps {
   int q;      // max read length
   int seeds;  // max seeds per strand

@@ -136,10 +136,51 @@ __global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix,
         if (lane == 0) {
           unsigned at = atomicAdd(b.n_ovf0, 1u);
           b.ovf0[at] = r;
+          b.reads[r] = mg_read_result{};  // not kReadUnscored: a later tier writes this read
         }
       }
       __syncwarp();
     }
+  }
+}
+
+// Scores of the reads the dual-strand tier left kReadUnscored, one thread per read: per candidate
+// CalculateScore's final arithmetic (MatrixCPU.cpp:209-212) and the relative score
+// (MatrixResult.cpp:21-29) from its raw sums, in place; then the strand merge and top group as
+// write_read_result_s (Analyser.cpp:592-611, 388). Kept apart from the warp-per-read kernel, this
+// double-precision arithmetic runs on full warps instead of one lane per candidate.
+__global__ void __launch_bounds__(256) k_finish_dual(DevIndex ix, BatchDev b, StageDev sd) {
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < b.n; r += (uint64_t)gridDim.x * blockDim.x) {
+    mg_read_result rr = b.reads[r];
+    if (rr.strand != kReadUnscored) continue;
+    const uint32_t L = (uint32_t)(b.offs[r + 1] - b.offs[r]);
+    const uint32_t n0 = rr.n_fwd, n1 = rr.n_rc, tot = n0 + n1;
+    mg_candidate* c = tot > (uint32_t)kSlots ? sd.arena + rr.cand_off : sd.stage + r * kSlots;
+    int err = 0;
+    float h0 = -1.0f, h1 = -1.0f;
+    for (uint32_t i = 0; i < tot; i++) {
+      const mg_candidate x = c[i];
+      float sc, pc;
+      final_score(__float_as_uint(x.rel), __float_as_uint(x.score), __float_as_uint(x.pct), L, &sc, &pc);
+      const float rl = relative_score_tab(ix, L, __ldg(ix.ref_len + x.ref), sc, &err);
+      c[i] = mg_candidate{x.ref, rl, sc, pc};
+      if (i < n0)
+        h0 = fmaxf(h0, rl);
+      else
+        h1 = fmaxf(h1, rl);
+    }
+    const int ch = h0 < h1 ? 1 : 0;  // Analyser.cpp:601
+    const uint32_t nch = ch ? n1 : n0;
+    const float hch = ch ? h1 : h0;
+    const mg_candidate* cc = c + (ch ? n0 : 0);
+    uint32_t top = 0;
+    for (uint32_t i = 0; i < nch; i++) top += cc[i].rel == hch;
+    rr.highest = hch;
+    rr.strand = (uint8_t)ch;
+    rr.reported = (nch > 0 && hch != 0.0f) ? 1 : 0;  // Analyser.cpp:388
+    rr.n_top = (uint16_t)top;
+    b.reads[r] = rr;
+    if (err) atomicOr(b.err, err);
   }
 }
 
@@ -743,6 +784,7 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       int per_sm1 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_classify_dual, kW1Warps * 32, 0);
       k_classify_dual<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      k_finish_dual<<<(unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8), 256, 0, st>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
       int per_sm2 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
