@@ -9,7 +9,9 @@
 //                      into its reference's entry; the longest run of ones is occMax
 //   rank sort          over the kept postings only, compacted first (usually about one per seed)
 // so the serial work per strand follows the kept postings, not all of them, and the two strands
-// run side by side. Nothing is indexed dynamically in registers; per-posting state lives in
+// run side by side. The kernel stops at the diagonal runs: the run ends of the references that can
+// become candidates leave as 16-byte records, and k_finish_dual (mg_lib.cu) walks, covers and
+// scores them one thread per read, work whose one-lane-per-run form would leave most lanes idle. Nothing is indexed dynamically in registers; per-posting state lives in
 // shared memory, whose regions are reused from step to step.
 #pragma once
 #include "mg_lean.cuh"
@@ -18,22 +20,17 @@ namespace mg {
 
 constexpr int kDualE = 64;               // postings per strand
 constexpr int kDualTab = 64;             // occurrence table entries per strand (>= distinct refs)
-constexpr int kDualC = 8;                // scored candidates per strand
-constexpr int kCovWords = kLeanQ / 32;   // coverage bitmap words per lane
 
 // Per-warp shared memory of the dual path; [half] = strand.
 struct DualSmem {
   uint32_t a[2][3][kDualE];     // gathered postings (ref, pos, found | seed << 8 | table entry << 16);
                                 // from the rank sort on: kept postings sorted (ref, pos, seed)
-  uint32_t c[2][3][kDualE];     // kept postings, compacted (ref, pos, seed); during scoring the
-                                // coverage bitmaps, kCovWords words per lane
+  uint32_t c[2][3][kDualE];     // kept postings, compacted (ref, pos, seed); at the end the run
+                                // records' refID, first-seed position and last-seed end
   uint32_t t[2][2][kDualTab];   // occurrence table (ref key, found mask, then occMax); from the
-                                // diagonal runs on: z (run ends) and segmax (reference heads)
-  mg_candidate cb[2][kDualC];   // scored candidates in ascending refID
+                                // diagonal runs on: the records' seed indices and segmax
   uint8_t q[2][kLeanQ];         // strand bases: forward, reverse complement
-  uint8_t q_pad[8];             // word reads of q[1]'s last bases run up to 7 bytes past it
 };
-static_assert(sizeof(uint32_t) * 2 * 3 * kDualE >= sizeof(uint32_t) * 32 * kCovWords, "coverage bitmaps");
 
 __device__ __forceinline__ unsigned long long upto64(int i) {  // bits 0..i
   return i >= 63 ? ~0ull : ((2ull << i) - 1ull);
@@ -42,39 +39,12 @@ __device__ __forceinline__ unsigned long long below64(int i) {  // bits 0..i-1
   return i <= 0 ? 0ull : upto64(i - 1);
 }
 
-// Four bytes from p (any alignment) as one little-endian word, read as two aligned words.
-__device__ __forceinline__ uint32_t bytes4(const uint8_t* p) {
-  const uintptr_t a = (uintptr_t)p;
-  const uint32_t* w = (const uint32_t*)(a & ~(uintptr_t)3);
-  return __funnelshift_r(w[0], w[1], (uint32_t)(a & 3) * 8u);
-}
-
-// tail_walk (mg_kernels.cuh) four bytes at a time: the length of the common prefix of the query
-// from lq and the reference from lr, at most min(rlen - lr, k, L - lq). Reads up to 7 bytes past
-// the last compared byte of each side (the index's base array and the strand buffers are padded).
-__device__ __forceinline__ uint32_t tail_walk4(const uint8_t* q, const uint8_t* rs, uint32_t L, uint32_t rlen,
-                                               uint32_t lq, uint32_t lr, uint32_t k) {
-  if (lq >= L || lr >= rlen) return 0;
-  const uint32_t lim = min(min(rlen - lr, k), L - lq);
-  for (uint32_t i = 0; i < lim; i += 4) {
-    const uint32_t x = bytes4(q + lq + i) ^ bytes4(rs + lr + i);
-    if (x) return min(i + ((uint32_t)(__ffs(x) - 1) >> 3), lim);
-  }
-  return lim;
-}
-
 // Bits of a full-warp ballot that belong to this lane's half.
 __device__ __forceinline__ uint32_t half_bits(uint32_t ballot, int sh) { return (ballot >> sh) & 0xFFFFu; }
 
-// A candidate before scoring: the sum of T(T+1)/2 over its scored runs, the sum of T and the
-// covered query bases, as the bits of the rel, score and pct fields.
-__device__ __forceinline__ mg_candidate raw_candidate(uint32_t ref, uint32_t sumr, uint32_t sumc, uint32_t hits) {
-  return mg_candidate{ref, __uint_as_float(sumr), __uint_as_float(sumc), __uint_as_float(hits)};
-}
-
 // Both strands of one read (bases already in S.q). Warp-uniform return: kStrandOk, or
 // kStrandOverflow when either strand does not fit. Each lane receives its half's strand result:
-// *n_out candidates in S.cb[half] (ascending refID), raw (raw_candidate).
+// *n_out run records (step 5) in S.c[half][0..2] and S.t[half][0], in ascending refID.
 __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_t* n_out) {
   const unsigned FULL = 0xffffffffu;
   const uint32_t EMPTY = 0xFFFFFFFFu;
@@ -204,7 +174,6 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
   }
   __syncwarp();
   // 4. diagonal runs over the sorted postings (Analyser.cpp:2337-2490)
-  uint32_t* z = S.t[half][0];
   uint32_t* segmax = S.t[half][1];
   auto brk = [&](int i) -> bool {
     if (i == 0) return true;
@@ -244,109 +213,40 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
   alive = alive && M >= 2;  // Analyser.cpp:2402
   if (!__any_sync(FULL, alive)) return kStrandOk;
   __syncwarp();
-  // 5. head/tail extension at every run end of a kept reference (runMax == M)
+  // 5. one record per run end of a kept reference whose longest run is M (the references that can
+  //    become candidates): refID, reference position of the run's first seed, reference end of its
+  //    last seed, the two seed indices. The head/tail walks, coverage and scores of these runs are
+  //    k_finish_dual's (one thread per read). The records go to shared memory regions free by now.
+  uint32_t* r_ref = S.c[half][0];
+  uint32_t* r_sr = S.c[half][1];
+  uint32_t* r_lr = S.c[half][2];
+  uint32_t* r_jj = S.t[half][0];
+  uint32_t nrec = 0;
   for (int s = 0; s < nkw; s++) {
     const int i = hl + 16 * s;
-    uint32_t zz = 0;
-    if (alive && i < (int)T2 && ((E >> i) & 1ull)) {
-      const int h = 63 - __clzll(R & upto64(i));
-      if (segmax[h] == (uint32_t)M) {
-        const int st = run_start(i);
-        const uint32_t ref = s_ref[i];
-        const uint32_t sr = s_pos[st], sq = s_j[st] * step;
-        const uint32_t lr = s_pos[i] + step, lq = s_j[i] * step + step;
-        const uint8_t* rs = ix.bases + ix.ref_off[ref];
-        const uint32_t rlen = ix.ref_len[ref];
-        const uint32_t tail = tail_walk4(q, rs, L, rlen, lq, lr, k);
-        const uint32_t head = head_walk(q, rs, sq, sr, k);
-        const uint32_t tot = tail + head + (lq - sq);
-        if (tot >= k) zz = ((sq - head) << 16) | tot;
-      }
+    const bool wk = alive && i < (int)T2 && ((E >> i) & 1ull) &&
+                    segmax[63 - __clzll(R & upto64(i))] == (uint32_t)M;
+    const uint32_t wb = half_bits(__ballot_sync(FULL, wk), sh);
+    if (wk) {
+      const uint32_t at = nrec + __popc(wb & ((1u << hl) - 1u));
+      const int st = run_start(i);
+      r_ref[at] = s_ref[i];
+      r_sr[at] = s_pos[st];
+      r_lr[at] = s_pos[i] + step;
+      r_jj[at] = s_j[st] | (s_j[i] << 8);
     }
-    if (i < (int)T2) z[i] = zz;
+    nrec += __popc(wb);
   }
   __syncwarp();
-  // 6. candidates: reference heads with runMax == M and a run end that scored (T >= k); their
-  //    output slots follow from the mask of candidate heads, in ascending refID
-  auto is_cand = [&](int h) -> bool {
-    if (!alive || h >= (int)T2 || !((R >> h) & 1ull) || segmax[h] != (uint32_t)M) return false;
-    const int se = seg_end(h);
-    for (int i = h; i <= se; i++)
-      if (z[i]) return true;
-    return false;
-  };
-  unsigned long long Sm = 0;
-  for (int s = 0; s < nkw; s++) Sm |= (unsigned long long)half_bits(__ballot_sync(FULL, is_cand(hl + 16 * s)), sh) << (16 * s);
-  const int n_sc = __popcll(Sm);
-  if (__any_sync(FULL, n_sc > kDualC)) return kStrandOverflow;
-  //    sums and coverage, one lane per candidate (MatrixCPU.cpp:18-208); the scores from them are
-  //    k_finish_dual's (MatrixCPU.cpp:209-212, MatrixResult.cpp:21-29)
-  const uint32_t nw = (L + 31) / 32;
-  uint32_t* cov = &S.c[0][0][0] + lane * kCovWords;
-  mg_candidate* cb = S.cb[half];
-  for (int s = 0; s < nkw; s++) {
-    const int h = hl + 16 * s;
-    if (!((Sm >> h) & 1ull)) continue;
-    const int se = seg_end(h);
-    for (uint32_t wd = 0; wd < nw; wd++) cov[wd] = 0;
-    uint32_t sumc = 0, sumr = 0;
-    for (int i = h; i <= se; i++) {
-      const uint32_t zz = z[i];
-      if (!zz) continue;
-      const uint32_t t = zz & 0xFFFFu, a = zz >> 16, b = a + t;
-      sumc += t;
-      sumr += t * (t + 1) / 2;
-      for (uint32_t wd = a >> 5; wd <= (b - 1) >> 5; wd++) {
-        const uint32_t w0 = wd * 32;
-        const uint32_t lo = a > w0 ? a : w0, up = b < w0 + 32 ? b : w0 + 32;
-        const uint32_t n = up - lo;
-        cov[wd] |= (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0);
-      }
-    }
-    uint32_t hits = 0;
-    for (uint32_t wd = 0; wd < nw; wd++) hits += __popc(cov[wd]);
-    cb[__popcll(Sm & below64(h))] = raw_candidate(s_ref[h], sumr, sumc, hits);
-  }
-  __syncwarp();
-  *n_out = (uint32_t)n_sc;
+  *n_out = nrec;
   return kStrandOk;
-}
-
-// The dual tier's read result: the raw candidates go to the read's staging slots (or the arena
-// when there are more than kSlots) and the read is marked kReadUnscored for k_finish_dual; a read
-// without candidates is final here (what write_read_result_s gives with no candidate).
-__device__ __forceinline__ void write_read_raw(const BatchDev& b, uint32_t r, uint32_t n0, uint32_t n1,
-                                               const mg_candidate* cb0, const mg_candidate* cb1, mg_candidate* stage,
-                                               mg_candidate* arena, uint64_t arena_cap, unsigned long long* arena_n,
-                                               int* errw) {
-  const uint32_t tot = n0 + n1;
-  if (tot == 0) {
-    b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
-    return;
-  }
-  uint32_t where = 0;
-  uint8_t mark = kReadUnscored;
-  mg_candidate* dst = stage + (uint64_t)r * kSlots;
-  if (tot > (uint32_t)kSlots) {
-    const unsigned long long at = atomicAdd(arena_n, (unsigned long long)tot);
-    if (at + tot > arena_cap) {  // the call grows the arena and runs the batch again
-      atomicOr(errw, kErrArena);
-      dst = nullptr;
-      mark = 0;
-    } else {
-      dst = arena + at;
-      where = (uint32_t)at;
-    }
-  }
-  if (dst) {
-    for (uint32_t c = 0; c < n0; c++) dst[c] = cb0[c];
-    for (uint32_t c = 0; c < n1; c++) dst[n0 + c] = cb1[c];
-  }
-  b.reads[r] = mg_read_result{-1.0f, where, (uint16_t)n0, (uint16_t)n1, mark, 0, 0};
 }
 
 // Read r on the dual path; false when it does not fit (the caller hands it on).
 // comp: the block's 256-entry table of complement(upper(byte)), 0 where there is none.
+// The read's run records (forward strand first) go to its staging slots, or to the arena when
+// there are more than kSlots, and the read is marked kReadUnscored for k_finish_dual; a read
+// without records is final here (no candidate).
 __device__ bool process_read_dual(const DevIndex& ix, const BatchDev& b, uint32_t r, DualSmem& S,
                                   const uint8_t* comp, mg_candidate* stage, mg_candidate* arena, uint64_t arena_cap,
                                   unsigned long long* arena_n, int* errw) {
@@ -366,15 +266,39 @@ __device__ bool process_read_dual(const DevIndex& ix, const BatchDev& b, uint32_
   }
   if (__any_sync(FULL, badl)) {
     if (lane == 0)
-      write_read_result_s(b, r, true, 0, 0, -1.0f, -1.0f, S.cb[0], S.cb[1], stage, arena, arena_cap, arena_n, errw, 0);
+      b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, MG_READ_BAD_BYTE, 0, 0};
+    if (lane == 0) atomicOr(errw, kErrBadInput);
     __syncwarp();
     return true;
   }
   __syncwarp();
   uint32_t nh;
   if (dual_strands(ix, L, S, &nh) != kStrandOk) return false;
-  const uint32_t n0 = __shfl_sync(FULL, nh, 0), n1 = __shfl_sync(FULL, nh, 16);
-  if (lane == 0) write_read_raw(b, r, n0, n1, S.cb[0], S.cb[1], stage, arena, arena_cap, arena_n, errw);
+  const uint32_t n0 = __shfl_sync(FULL, nh, 0), n1 = __shfl_sync(FULL, nh, 16), tot = n0 + n1;
+  if (tot == 0) {
+    if (lane == 0) b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, 0, 0, 0};
+    __syncwarp();
+    return true;
+  }
+  unsigned long long at = 0;
+  if (lane == 0 && tot > (uint32_t)kSlots) at = atomicAdd(arena_n, (unsigned long long)tot);
+  at = __shfl_sync(FULL, at, 0);
+  const bool big = tot > (uint32_t)kSlots;
+  const bool fits = !big || at + tot <= arena_cap;  // else the call grows the arena and runs again
+  if (fits) {
+    mg_candidate* dst = big ? arena + at : stage + (uint64_t)r * kSlots;
+    for (uint32_t x = lane; x < tot; x += 32) {
+      const int h = x >= n0 ? 1 : 0;
+      const uint32_t i = x - (h ? n0 : 0);
+      dst[x] = mg_candidate{S.c[h][0][i], __uint_as_float(S.c[h][1][i]), __uint_as_float(S.c[h][2][i]),
+                            __uint_as_float(S.t[h][0][i])};
+    }
+  }
+  if (lane == 0) {
+    if (!fits) atomicOr(errw, kErrArena);
+    b.reads[r] = mg_read_result{-1.0f, big ? (uint32_t)at : 0u, (uint16_t)n0, (uint16_t)n1,
+                                fits ? kReadUnscored : (uint8_t)0, 0, 0};
+  }
   __syncwarp();
   return true;
 }

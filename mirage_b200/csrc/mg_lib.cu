@@ -144,41 +144,103 @@ __global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix,
   }
 }
 
-// Scores of the reads the dual-strand tier left kReadUnscored, one thread per read: per candidate
-// CalculateScore's final arithmetic (MatrixCPU.cpp:209-212) and the relative score
-// (MatrixResult.cpp:21-29) from its raw sums, in place; then the strand merge and top group as
-// write_read_result_s (Analyser.cpp:592-611, 388). Kept apart from the warp-per-read kernel, this
-// double-precision arithmetic runs on full warps instead of one lane per candidate.
-__global__ void __launch_bounds__(256) k_finish_dual(DevIndex ix, BatchDev b, StageDev sd) {
+// Finishing pass of the dual-strand tier, one thread per read it left kReadUnscored. The read's
+// run records (forward strand first, each strand in ascending refID; see process_read_dual) name
+// the run ends of the references whose longest run is M. Per record the head and tail walks
+// (head_walk, tail_walk) on the strand's bases, read from the batch: forward in upper case, the
+// reverse complement backwards through the complement table. Per reference the runs that scored
+// (T >= k) give the sums and the query coverage; a reference with such a run is a candidate:
+// Score, percentage and relative score (MatrixCPU.cpp:18-214, MatrixResult.cpp:21-29) replace its
+// records, compacted in place. Then the strand merge and top group as write_read_result_s
+// (Analyser.cpp:592-611, 388). One thread per read keeps every lane busy where the warp-per-read
+// kernel would run this one lane per run end.
+constexpr int kFinThreads = 256;
+constexpr int kCovStride = kLeanQ / 32 + 1;  // coverage words per thread; odd, so no bank conflicts
+
+__global__ void __launch_bounds__(kFinThreads) k_finish_dual(DevIndex ix, BatchDev b, StageDev sd) {
+  __shared__ uint8_t comp[256];
+  __shared__ uint32_t covs[kFinThreads * kCovStride];
+  for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
+  __syncthreads();
+  uint32_t* cov = covs + threadIdx.x * kCovStride;
+  const uint32_t k = (uint32_t)ix.k, step = (uint32_t)ix.step;
   for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < b.n; r += (uint64_t)gridDim.x * blockDim.x) {
     mg_read_result rr = b.reads[r];
     if (rr.strand != kReadUnscored) continue;
-    const uint32_t L = (uint32_t)(b.offs[r + 1] - b.offs[r]);
-    const uint32_t n0 = rr.n_fwd, n1 = rr.n_rc, tot = n0 + n1;
-    mg_candidate* c = tot > (uint32_t)kSlots ? sd.arena + rr.cand_off : sd.stage + r * kSlots;
+    const uint64_t o0 = b.offs[r];
+    const uint32_t L = (uint32_t)(b.offs[r + 1] - o0);
+    const uint8_t* raw = b.bases + o0;
+    const uint32_t n0 = rr.n_fwd, nrec = n0 + rr.n_rc;
+    const bool big = nrec > (uint32_t)kSlots;
+    mg_candidate* rec = big ? sd.arena + rr.cand_off : sd.stage + r * kSlots;
+    const uint32_t nw = (L + 31) / 32;
     int err = 0;
-    float h0 = -1.0f, h1 = -1.0f;
-    for (uint32_t i = 0; i < tot; i++) {
-      const mg_candidate x = c[i];
-      float sc, pc;
-      final_score(__float_as_uint(x.rel), __float_as_uint(x.score), __float_as_uint(x.pct), L, &sc, &pc);
-      const float rl = relative_score_tab(ix, L, __ldg(ix.ref_len + x.ref), sc, &err);
-      c[i] = mg_candidate{x.ref, rl, sc, pc};
-      if (i < n0)
-        h0 = fmaxf(h0, rl);
-      else
-        h1 = fmaxf(h1, rl);
+    float hi[2] = {-1.0f, -1.0f};
+    uint32_t nc[2] = {0, 0}, out = 0;
+    for (int strand = 0; strand < 2; strand++) {
+      auto qb = [&](uint32_t x) -> uint8_t { return strand ? comp[raw[L - 1 - x]] : upper_dev(raw[x]); };
+      const uint32_t end = strand ? nrec : n0;
+      for (uint32_t g = strand ? n0 : 0; g < end;) {
+        const uint32_t ref = rec[g].ref;
+        const uint8_t* rs = ix.bases + ix.ref_off[ref];
+        const uint32_t rlen = ix.ref_len[ref];
+        uint32_t sumc = 0, sumr = 0, nsc = 0, e = g;
+        for (; e < end && rec[e].ref == ref; e++) {
+          const mg_candidate x = rec[e];
+          const uint32_t sr = __float_as_uint(x.rel), lr = __float_as_uint(x.score), jj = __float_as_uint(x.pct);
+          const uint32_t sq = (jj & 0xFFu) * step, lq = (jj >> 8) * step + step;
+          uint32_t tail = 0;  // tail_walk
+          if (lq < L && lr < rlen) {
+            const uint32_t lim = min(min(rlen - lr, k), L - lq);
+            while (tail < lim && qb(lq + tail) == rs[lr + tail]) tail++;
+          }
+          uint32_t head = 0;  // head_walk
+          const uint32_t hsz = min(sr, k);
+          if (sq != 0 && hsz != 0) {
+            const uint32_t jb = min(sq - 1, hsz - 1);
+            while (head < jb && qb(sq - 1 - head) == rs[sr - head]) head++;
+          }
+          const uint32_t tot = tail + head + (lq - sq);
+          if (tot < k) continue;
+          if (nsc++ == 0)
+            for (uint32_t wd = 0; wd < nw; wd++) cov[wd] = 0;
+          sumc += tot;
+          sumr += tot * (tot + 1) / 2;
+          const uint32_t a = sq - head, bnd = a + tot;
+          for (uint32_t wd = a >> 5; wd <= (bnd - 1) >> 5; wd++) {
+            const uint32_t w0 = wd * 32;
+            const uint32_t lo = a > w0 ? a : w0, up = bnd < w0 + 32 ? bnd : w0 + 32;
+            const uint32_t n = up - lo;
+            cov[wd] |= (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0);
+          }
+        }
+        if (nsc) {
+          uint32_t hits = 0;
+          for (uint32_t wd = 0; wd < nw; wd++) hits += __popc(cov[wd]);
+          float sc, pc;
+          final_score(sumr, sumc, hits, L, &sc, &pc);
+          const float rl = relative_score_tab(ix, L, rlen, sc, &err);
+          rec[out++] = mg_candidate{ref, rl, sc, pc};  // out <= g: this group's records are read
+          nc[strand]++;
+          hi[strand] = fmaxf(hi[strand], rl);
+        }
+        g = e;
+      }
     }
-    const int ch = h0 < h1 ? 1 : 0;  // Analyser.cpp:601
-    const uint32_t nch = ch ? n1 : n0;
-    const float hch = ch ? h1 : h0;
-    const mg_candidate* cc = c + (ch ? n0 : 0);
+    const uint32_t tot = nc[0] + nc[1];
+    mg_candidate* fin = rec;
+    if (big && tot <= (uint32_t)kSlots) {  // k_scatter takes up to kSlots candidates from the slots
+      fin = sd.stage + r * kSlots;
+      for (uint32_t c = 0; c < tot; c++) fin[c] = rec[c];
+    }
+    const int ch = hi[0] < hi[1] ? 1 : 0;  // Analyser.cpp:601
+    const uint32_t nch = nc[ch];
+    const float hch = hi[ch];
+    const mg_candidate* cc = fin + (ch ? nc[0] : 0);
     uint32_t top = 0;
     for (uint32_t i = 0; i < nch; i++) top += cc[i].rel == hch;
-    rr.highest = hch;
-    rr.strand = (uint8_t)ch;
-    rr.reported = (nch > 0 && hch != 0.0f) ? 1 : 0;  // Analyser.cpp:388
-    rr.n_top = (uint16_t)top;
+    rr = mg_read_result{hch, tot > (uint32_t)kSlots ? rr.cand_off : 0u, (uint16_t)nc[0], (uint16_t)nc[1], (uint8_t)ch,
+                        (uint8_t)((nch > 0 && hch != 0.0f) ? 1 : 0), (uint16_t)top};  // reported: Analyser.cpp:388
     b.reads[r] = rr;
     if (err) atomicOr(b.err, err);
   }
@@ -784,7 +846,8 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       int per_sm1 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_classify_dual, kW1Warps * 32, 0);
       k_classify_dual<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
-      k_finish_dual<<<(unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8), 256, 0, st>>>(ix->dix, b, sd);
+      k_finish_dual<<<(unsigned)std::min<uint64_t>((n + kFinThreads - 1) / kFinThreads, (uint64_t)sms * 8), kFinThreads, 0,
+                      st>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
       int per_sm2 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
