@@ -22,7 +22,7 @@ constexpr int kDualE = 64;               // postings per strand
 constexpr int kDualTab = 64;             // occurrence table entries per strand (>= distinct refs)
 
 // Per-warp shared memory of the dual path; [half] = strand.
-struct DualSmem {
+struct alignas(16) DualSmem {  // 16-byte aligned: the table clear stores 16 bytes a lane
   uint32_t a[2][3][kDualE];     // gathered postings (ref, pos, found | seed << 8 | table entry << 16);
                                 // from the rank sort on: kept postings sorted (ref, pos, seed)
   uint32_t c[2][3][kDualE];     // kept postings, compacted (ref, pos, seed); at the end the run
@@ -98,10 +98,9 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
   if (!__any_sync(FULL, alive)) return kStrandOk;
   // 2. occurrence filter (Analyser.cpp:2057-2115): per reference, the found indices where it
   //    occurs (a table keyed by refID); the longest run of consecutive ones is its occMax
-  for (int x = hl; x < kDualTab; x += 16) {
-    tkey[x] = EMPTY;
-    tval[x] = 0;
-  }
+  static_assert(kDualTab == 64, "the table clear below covers 64 entries with 16 lanes");
+  reinterpret_cast<uint4*>(tkey)[hl] = make_uint4(EMPTY, EMPTY, EMPTY, EMPTY);
+  reinterpret_cast<uint4*>(tval)[hl] = make_uint4(0u, 0u, 0u, 0u);
   __syncwarp();
   const int nslw = (int)__reduce_max_sync(FULL, (T + 15) / 16);  // posting blocks, warp-uniform
   for (int s = 0; s < nslw; s++) {
