@@ -148,12 +148,29 @@ __global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix,
 // run records (forward strand first, each strand in ascending refID; see process_read_dual) name
 // the run ends of the references whose longest run is M. Per record the head and tail walks
 // (head_walk, tail_walk) on the strand's bases, read from the batch: forward in upper case, the
-// reverse complement backwards through the complement table. Per reference the runs that scored
+// reverse complement backwards through the complement table; the tail four bytes at a time while
+// the window has four left. Per reference the runs that scored
 // (T >= k) give the sums and the query coverage; a reference with such a run is a candidate:
 // Score, percentage and relative score (MatrixCPU.cpp:18-214, MatrixResult.cpp:21-29) replace its
 // records, compacted in place. Then the strand merge and top group as write_read_result_s
 // (Analyser.cpp:592-611, 388). One thread per read keeps every lane busy where the warp-per-read
 // kernel would run this one lane per run end.
+// Four bytes p..p+3, all readable, as one little-endian word: the aligned word holding p and,
+// only when p is not 4-aligned, the next aligned word (which holds p+3), so nothing outside
+// p..p+3's words is read.
+__device__ __forceinline__ uint32_t load4(const uint8_t* p) {
+  const uintptr_t a = (uintptr_t)p;
+  const uint32_t* w = (const uint32_t*)(a & ~(uintptr_t)3);
+  const uint32_t sh = (uint32_t)(a & 3u);
+  const uint32_t lo = w[0];
+  return sh ? __funnelshift_r(lo, w[1], sh * 8u) : lo;
+}
+// upper_dev on each byte of w: bytes 0x61..0x7F lose 0x20.
+__device__ __forceinline__ uint32_t upper4(uint32_t w) {
+  const uint32_t m = (((w & 0x7F7F7F7Fu) + 0x1F1F1F1Fu) & ~w) & 0x80808080u;
+  return w - (m >> 2);
+}
+
 constexpr int kFinThreads = 256;
 constexpr int kCovStride = kLeanQ / 32 + 1;  // coverage words per thread; odd, so no bank conflicts
 
@@ -192,6 +209,19 @@ __global__ void __launch_bounds__(kFinThreads) k_finish_dual(DevIndex ix, BatchD
           uint32_t tail = 0;  // tail_walk
           if (lq < L && lr < rlen) {
             const uint32_t lim = min(min(rlen - lr, k), L - lq);
+            while (tail + 4 <= lim) {  // four bytes at a time while all four are in the window
+              uint32_t wq;
+              if (strand) {
+                const uint32_t w = load4(raw + (L - 4 - (lq + tail)));
+                wq = (uint32_t)comp[w >> 24] | ((uint32_t)comp[(w >> 16) & 0xFFu] << 8) |
+                     ((uint32_t)comp[(w >> 8) & 0xFFu] << 16) | ((uint32_t)comp[w & 0xFFu] << 24);
+              } else {
+                wq = upper4(load4(raw + lq + tail));
+              }
+              const uint32_t x = wq ^ load4(rs + lr + tail);
+              if (x) break;
+              tail += 4;
+            }
             while (tail < lim && qb(lq + tail) == rs[lr + tail]) tail++;
           }
           uint32_t head = 0;  // head_walk
