@@ -128,9 +128,11 @@ int mg_eval_logf(mg_index* ix, const float* x, float* out, uint64_t n);
 
 /* Diagnostics (no counterpart in the reference). mg_set_timing(ix, 1) records CUDA events
  * around every kernel of each following classification call; mg_last_kernel_times writes the
- * last call's device times in milliseconds, 5 entries: [dual-strand warp tier (or the plain
- * form's kernel), general warp tier, block tier, global-memory tier, output compaction]. mg_bucket_sizes returns the number of postings stored under each of n 28-bit
- * hashes (the index directory, read on the device). */
+ * last call's device times in milliseconds, 5 entries: [dual-strand warp tier with its finishing
+ * pass (or the plain form's kernel), general warp tier, block tier, global-memory tier, output
+ * compaction]; in the batched and served forms the second to fourth run on a second stream,
+ * beside the finishing pass. mg_bucket_sizes returns the number of postings stored under each
+ * of n 28-bit hashes (the index directory, read on the device). */
 int mg_set_timing(mg_index* ix, int on);
 /* Diagnostic (no counterpart in the reference): the roofline of the lookup path. Times 2^26
  * gathers of whole 32-byte sectors (8 lanes per sector) at pseudo-random positions of a device

@@ -38,8 +38,17 @@ struct DevBuf {
 // Device buffers of one classification call in flight (a call owns one at a time).
 struct Workspace {
   DevBuf offs, bases, reads, stage, arena, cands, ctr, ovf, sums, gws, chain;
+  // the stream on which the tiers after the dual tier run beside its finishing pass, and the
+  // events that fork it from and join it back to the call's stream (made at first use)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   void release() {
     for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws, &chain}) b->release();
+    if (side) cudaStreamDestroy(side);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    side = nullptr;
+    fork = join = nullptr;
   }
   size_t bytes() const {
     return offs.n + bases.n + reads.n + stage.n + arena.n + cands.n + ctr.n + ovf.n + sums.n + gws.n + chain.n;
@@ -103,7 +112,7 @@ struct mg_index {
   // optional per-kernel timing of the last pipeline (events on the launching stream)
   bool timing = false;
   bool events_made = false;
-  cudaEvent_t ev[6];
+  cudaEvent_t ev[8];
   // arguments of the last mg_classify_device launch, for its completion in the sync call
   struct {
     uint64_t n = 0, cap = 0;

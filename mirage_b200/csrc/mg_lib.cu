@@ -864,34 +864,56 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   }
   const bool tm = ix->timing && ix->events_made;
   if (n > 0) {
+    // timing events (start, end) per tier: ev[0..1] first tier, ev[2..3] general warp tier,
+    // ev[3..4] block tier, ev[4..5] global tier, ev[6..7] compaction
     if (tm) CU(cudaEventRecord(ix->ev[0], st));
+    auto global_tier = [&](cudaStream_t s) {
+      k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, s>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3, nullptr,
+                                                                    nullptr, w.gws.as<uint8_t>(), l3, c3, 1);
+    };
     if (plain) {
       // every read gets its own block (one launch for the batch)
       k_classify_block<kB2Threads><<<(unsigned)n, kB2Threads, l2.total, st>>>(
           ix->dix, b, sd, nullptr, nullptr, nullptr, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
-      if (tm) CU(cudaEventRecord(ix->ev[1], st));
-      if (tm) CU(cudaEventRecord(ix->ev[2], st));
-      if (tm) CU(cudaEventRecord(ix->ev[3], st));
+      if (tm) {
+        CU(cudaEventRecord(ix->ev[1], st));
+        CU(cudaEventRecord(ix->ev[2], st));
+        CU(cudaEventRecord(ix->ev[3], st));
+        CU(cudaEventRecord(ix->ev[4], st));
+      }
+      global_tier(st);
+      if (tm) CU(cudaEventRecord(ix->ev[5], st));
     } else {
+      if (!w.side) {
+        CU(cudaStreamCreateWithFlags(&w.side, cudaStreamNonBlocking));
+        CU(cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&w.join, cudaEventDisableTiming));
+      }
       int per_sm1 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_classify_dual, kW1Warps * 32, 0);
       k_classify_dual<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
+      // the reads the dual tier handed on go through the other tiers on the side stream, beside
+      // the dual tier's finishing pass (different reads, disjoint slots; arena space by atomics)
+      CU(cudaEventRecord(w.fork, st));
+      CU(cudaStreamWaitEvent(w.side, w.fork, 0));
+      if (tm) CU(cudaEventRecord(ix->ev[2], w.side));
+      int per_sm2 = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
+      k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, w.side>>>(ix->dix, b, sd);
+      if (tm) CU(cudaEventRecord(ix->ev[3], w.side));
+      k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, w.side>>>(
+          ix->dix, b, sd, b.ovf1, b.n_ovf1, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
+      if (tm) CU(cudaEventRecord(ix->ev[4], w.side));
+      global_tier(w.side);
+      if (tm) CU(cudaEventRecord(ix->ev[5], w.side));
+      CU(cudaEventRecord(w.join, w.side));
       k_finish_dual<<<(unsigned)std::min<uint64_t>((n + kFinThreads - 1) / kFinThreads, (uint64_t)sms * 8), kFinThreads, 0,
                       st>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
-      int per_sm2 = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
-      k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
-      if (tm) CU(cudaEventRecord(ix->ev[2], st));
-      k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, st>>>(
-          ix->dix, b, sd, b.ovf1, b.n_ovf1, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
-      if (tm) CU(cudaEventRecord(ix->ev[3], st));
+      CU(cudaStreamWaitEvent(st, w.join, 0));
     }
     CU(cudaGetLastError());
-    k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, st>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3,
-                                                                   nullptr, nullptr, w.gws.as<uint8_t>(), l3, c3, 1);
-    if (tm) CU(cudaEventRecord(ix->ev[4], st));
-    CU(cudaGetLastError());
+    if (tm) CU(cudaEventRecord(ix->ev[6], st));
     const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
     unsigned long long* sums = w.sums.as<unsigned long long>();
     k_count_sums<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums);
@@ -900,7 +922,7 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
     if (cs && cs->snap) CU(cudaMemcpyAsync(cs->snap, chain, 8, cudaMemcpyDeviceToHost, st));
     if (cs && cs->scanned) CU(cudaEventRecord(cs->scanned, st));
     k_scatter<<<(unsigned)nb, kScanBlock, 0, st>>>(d_reads, n, sums, sd, d_out, cap, b.err);
-    if (tm) CU(cudaEventRecord(ix->ev[5], st));
+    if (tm) CU(cudaEventRecord(ix->ev[7], st));
     CU(cudaGetLastError());
   }
   return MG_OK;
@@ -1238,9 +1260,10 @@ int mg_set_timing(mg_index* ix, int on) {
 int mg_last_kernel_times(mg_index* ix, float* ms) {
   if (!ix || !ms) return set_error(MG_ERR_INVAL, "null argument");
   if (!ix->timing || !ix->events_made) return set_error(MG_ERR_INVAL, "timing is off");
+  static const int from[5] = {0, 2, 3, 4, 6}, to[5] = {1, 3, 4, 5, 7};
   for (int i = 0; i < 5; i++) {
-    CU(cudaEventSynchronize(ix->ev[i + 1]));
-    CU(cudaEventElapsedTime(&ms[i], ix->ev[i], ix->ev[i + 1]));
+    CU(cudaEventSynchronize(ix->ev[to[i]]));
+    CU(cudaEventElapsedTime(&ms[i], ix->ev[from[i]], ix->ev[to[i]]));
   }
   return MG_OK;
 }
