@@ -969,9 +969,10 @@ int error_status(int err) {
   return MG_OK;
 }
 
-// Reads per chunk of the batched form with host buffers; a batch of fewer than twice this runs
-// in one piece.
-constexpr uint64_t kChunkReads = 131072;
+// Smallest chunk of the batched form with host buffers: a batch of fewer than twice this runs in
+// one piece, and from kMaxChunks times this on the chunks are weighted (1,000,000 reads: 8
+// chunks, the first and last 55,556 reads).
+constexpr uint64_t kChunkReads = 65536;
 constexpr int kRunWhole = 1;
 
 // Batched form with host buffers, in chunks: chunk i's offsets and bases are copied on the index's h2d stream

@@ -145,12 +145,14 @@ def _same(a, b):
     assert np.array_equal(a.cands.view(np.uint8), b.cands.view(np.uint8))
 
 
-def test_chunked_batch_equals_one_piece(golden):
+@pytest.mark.parametrize("copies", [100, 200])
+def test_chunked_batch_equals_one_piece(golden, copies):
     """A batch large enough for the chunked form (copies overlapped with classification, candidate
-    offsets continued across chunks) equals the plain form and repeats the golden results."""
+    offsets continued across chunks) equals the plain form and repeats the golden results:
+    300,000 reads in 4 equal chunks, 600,000 reads in 8 chunks of weighted sizes."""
     g = golden("uneven_small")
     gix = M.Index(g.image)
-    data, offs = _tile(g.reads.data, g.reads.offs, 100)
+    data, offs = _tile(g.reads.data, g.reads.offs, copies)
     big = gix.classify(data, offs)
     _same(big, gix.classify(data, offs, form="plain"))
     one = gix.classify(g.reads.data, g.reads.offs)
