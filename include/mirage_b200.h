@@ -181,7 +181,9 @@ int mg_score_batch(mg_index* ix, const mg_batch* batch, mg_result* out);
 int mg_classify(mg_index* ix, const mg_batch* batch, mg_result* out);
 
 /* Batched form on device-resident buffers (no host copies): d_offsets / d_bases / outputs are
- * device pointers; stream is a cudaStream_t (NULL = the index's stream). */
+ * device pointers; stream is a cudaStream_t (NULL = the index's stream). Part of the work runs
+ * on a second, internal stream that waits for `stream` and that `stream` waits for again before
+ * the results are written, so work queued on `stream` before and after sees the usual order. */
 int mg_classify_device(mg_index* ix, uint64_t n_reads, const uint64_t* d_offsets,
                        const uint8_t* d_bases, mg_read_result* d_reads, mg_candidate* d_cands,
                        uint64_t cand_cap, uint64_t* d_n_cands, void* stream);
