@@ -112,8 +112,8 @@ static void slot_free(Slot& s) {
   s.ws.release();
 }
 
-// Form a step from the queue (server lock held) and launch it on the slot's stream.
-static void form_step(mg_server* sv, Slot& s) {
+// Take a step's worth of request segments from the queue (server lock held).
+static void carve_step(mg_server* sv, Slot& s) {
   s.parts.clear();
   s.n = 0;
   uint64_t nb = 0;
@@ -141,7 +141,14 @@ static void form_step(mg_server* sv, Slot& s) {
   }
   s.busy = true;
   s.launch_rc = MG_OK;
+}
+
+// Copy a carved step's segments from the ring and launch it on the slot's stream (server lock not
+// held: the segments' requests stay queued-or-running, so their ring memory stays in place).
+static void launch_step(mg_server* sv, Slot& s) {
   if (s.n == 0) return;
+  uint64_t nb = 0;
+  for (const Part& p : s.parts) nb += p.req->offs[p.first + p.count] - p.req->offs[p.first];
   if (slot_alloc(s, s.n, std::max<uint64_t>(nb, sv->step_bases), std::max<uint64_t>(s.cap_cands, 16 * s.n + 1024))) {
     s.launch_rc = MG_ERR_OOM;
     return;
@@ -208,7 +215,8 @@ static void drain_step(mg_server* sv, Slot& s) {
         cudaStreamSynchronize(s.st) != cudaSuccess)
       rc = set_error(MG_ERR_CUDA, "step results");
   }
-  std::lock_guard<std::mutex> lk(sv->mu);
+  // results to the requests without the lock: until a request completes, only this thread
+  // writes its result vectors and error code
   uint64_t at = 0;
   for (const Part& p : s.parts) {
     Request* r = p.req;
@@ -232,8 +240,12 @@ static void drain_step(mg_server* sv, Slot& s) {
         dst[i] = rr;
       }
     }
-    r->done += p.count;
     at += p.count;
+  }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  for (const Part& p : s.parts) {
+    Request* r = p.req;
+    r->done += p.count;
     if (r->done == r->n) {
       r->complete = true;
       if (!r->released) {
@@ -257,7 +269,12 @@ static void server_loop(mg_server* sv) {
     // launch into every free slot while there is work (asynchronous)
     for (int i = 0; i < 2; i++) {
       Slot& s = sv->slot[(oldest + i) % 2];
-      if (!s.busy && !sv->queue.empty()) form_step(sv, s);
+      if (!s.busy && !sv->queue.empty()) {
+        carve_step(sv, s);
+        lk.unlock();
+        launch_step(sv, s);
+        lk.lock();
+      }
     }
     // drain the oldest busy slot
     Slot* d = nullptr;
@@ -360,28 +377,32 @@ int mg_server_submit(mg_server* sv, const mg_batch* b, uint64_t* ticket) {
   return MG_OK;
 }
 
-static int take_result(mg_server* sv, std::map<uint64_t, std::unique_ptr<Request>>::iterator it, mg_result* out) {
-  Request* r = it->second.get();
-  if (r->error) {
-    int e = r->error;
-    sv->live.erase(it);
-    return set_error(e, mg_strerror(e));
+// Hand a completed request to its caller: detached from the server under the lock, copied out and
+// freed after the lock is released. A request whose candidates do not fit stays for a retry.
+static int take_result(mg_server* sv, std::map<uint64_t, std::unique_ptr<Request>>::iterator it, mg_result* out,
+                       std::unique_lock<std::mutex>& lk) {
+  Request* r0 = it->second.get();
+  if (!r0->error && r0->cands.size() > out->cand_cap) {
+    out->n_cands = r0->cands.size();
+    return set_error(MG_ERR_OOM, "candidate output buffer too small");
   }
+  std::unique_ptr<Request> r = std::move(it->second);
+  sv->live.erase(it);
+  lk.unlock();
+  if (r->error) return set_error(r->error, mg_strerror(r->error));
   out->n_cands = r->cands.size();
-  if (r->cands.size() > out->cand_cap) return set_error(MG_ERR_OOM, "candidate output buffer too small");
   if (r->n) std::memcpy(out->reads, r->reads.data(), r->n * sizeof(mg_read_result));
   if (!r->cands.empty()) std::memcpy(out->cands, r->cands.data(), r->cands.size() * sizeof(mg_candidate));
-  sv->live.erase(it);
   return 1;
 }
 
 int mg_server_poll(mg_server* sv, uint64_t ticket, mg_result* out) {
   if (!sv || !out) return set_error(MG_ERR_INVAL, "null argument");
-  std::lock_guard<std::mutex> lk(sv->mu);
+  std::unique_lock<std::mutex> lk(sv->mu);
   auto it = sv->live.find(ticket);
   if (it == sv->live.end()) return set_error(MG_ERR_INVAL, "unknown ticket");
   if (!it->second->complete) return 0;
-  return take_result(sv, it, out);
+  return take_result(sv, it, out, lk);
 }
 
 int mg_server_wait(mg_server* sv, uint64_t ticket, mg_result* out, uint32_t timeout_ms) {
@@ -392,7 +413,7 @@ int mg_server_wait(mg_server* sv, uint64_t ticket, mg_result* out, uint32_t time
   Request* r = it->second.get();
   if (!sv->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return r->complete; }))
     return set_error(MG_ERR_TIMEOUT, "request not complete within the timeout");
-  return take_result(sv, sv->live.find(ticket), out);
+  return take_result(sv, sv->live.find(ticket), out, lk);
 }
 
 void mg_server_destroy(mg_server* sv) {
