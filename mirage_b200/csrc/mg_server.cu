@@ -215,32 +215,68 @@ static void drain_step(mg_server* sv, Slot& s) {
         cudaStreamSynchronize(s.st) != cudaSuccess)
       rc = set_error(MG_ERR_CUDA, "step results");
   }
-  // results to the requests without the lock: until a request completes, only this thread
-  // writes its result vectors and error code
-  uint64_t at = 0;
-  for (const Part& p : s.parts) {
+  // results to the requests without the lock: until a request completes, only the server writes
+  // its result vectors and error code, and a step holds at most one segment of each request, so
+  // the segments can be delivered in parallel
+  auto deliver = [&](const Part& p, uint64_t at) {
     Request* r = p.req;
     if (rc != MG_OK) {
       r->error = rc;
-    } else if (!r->error) {
-      // the segment's candidates are contiguous in the step's output (read order): one copy
-      const mg_read_result* src = s.h_reads + at;
-      const mg_read_result& last = src[p.count - 1];
-      const uint64_t c0 = src[0].cand_off, c1 = (uint64_t)last.cand_off + last.n_fwd + last.n_rc;
-      const uint64_t base = r->cands.size();
+      return;
+    }
+    if (r->error) return;
+    // the segment's candidates are contiguous in the step's output (read order): one copy
+    const mg_read_result* src = s.h_reads + at;
+    const mg_read_result& last = src[p.count - 1];
+    const uint64_t c0 = src[0].cand_off, c1 = (uint64_t)last.cand_off + last.n_fwd + last.n_rc;
+    const uint64_t base = r->cands.size();
+    try {
       r->cands.insert(r->cands.end(), s.h_cands + c0, s.h_cands + c1);
-      mg_read_result* dst = r->reads.data() + p.first;
-      for (uint64_t i = 0; i < p.count; i++) {
-        mg_read_result rr = src[i];
-        if (rr.strand == MG_READ_BAD_BYTE || rr.strand == MG_READ_TOO_LARGE) {
-          r->error = rr.strand == MG_READ_BAD_BYTE ? MG_ERR_BADINPUT : MG_ERR_LIMIT;
-          break;
-        }
-        rr.cand_off = (uint32_t)(rr.cand_off - c0 + base);
-        dst[i] = rr;
+    } catch (...) {
+      r->error = MG_ERR_OOM;
+      return;
+    }
+    mg_read_result* dst = r->reads.data() + p.first;
+    for (uint64_t i = 0; i < p.count; i++) {
+      mg_read_result rr = src[i];
+      if (rr.strand == MG_READ_BAD_BYTE || rr.strand == MG_READ_TOO_LARGE) {
+        r->error = rr.strand == MG_READ_BAD_BYTE ? MG_ERR_BADINPUT : MG_ERR_LIMIT;
+        break;
+      }
+      rr.cand_off = (uint32_t)(rr.cand_off - c0 + base);
+      dst[i] = rr;
+    }
+  };
+  const size_t np = s.parts.size();
+  std::vector<uint64_t> start(np + 1, 0);
+  for (size_t i = 0; i < np; i++) start[i + 1] = start[i] + s.parts[i].count;
+  auto deliver_range = [&](size_t a, size_t b) {
+    for (size_t i = a; i < b; i++) deliver(s.parts[i], start[i]);
+  };
+  // large steps: up to kDeliverThreads contiguous ranges of segments with about equal reads
+  constexpr int kDeliverThreads = 4;
+  constexpr uint64_t kDeliverMin = 32768;  // reads per helper thread worth its start-up
+  const int nt = (int)std::min<uint64_t>({(uint64_t)kDeliverThreads, (uint64_t)np, s.n / kDeliverMin});
+  if (nt <= 1) {
+    deliver_range(0, np);
+  } else {
+    std::vector<size_t> cut(nt + 1, np);
+    cut[0] = 0;
+    for (int t = 1, i = 0; t < nt; t++) {
+      const uint64_t want = s.n * (uint64_t)t / (uint64_t)nt;
+      while ((size_t)i < np && start[i] < want) i++;
+      cut[t] = std::max<size_t>(cut[t - 1], (size_t)i);
+    }
+    std::vector<std::thread> helpers;
+    for (int t = 1; t < nt; t++) {
+      try {
+        helpers.emplace_back(deliver_range, cut[t], cut[t + 1]);
+      } catch (...) {  // no thread: deliver this range here
+        deliver_range(cut[t], cut[t + 1]);
       }
     }
-    at += p.count;
+    deliver_range(cut[0], cut[1]);
+    for (std::thread& h : helpers) h.join();
   }
   std::lock_guard<std::mutex> lk(sv->mu);
   for (const Part& p : s.parts) {
