@@ -45,9 +45,9 @@ sys.path.insert(0, ROOT)
 
 SEED = 2024
 N_READS = 1_000_000
-# kernels one batched call launches: dual-strand warp tier, its scoring pass, general warp tier,
-# block tier, global tier, candidate count, scan, scatter
-LAUNCHES_PER_BATCH = 8
+# kernels one batched call launches: dual-strand tier, second dual-strand tier (its leftovers),
+# the finishing pass, general warp tier, block tier, global tier, candidate count, scan, scatter
+LAUNCHES_PER_BATCH = 9
 # DRAM bytes (read + write) of one k_classify_dual launch on the default workload (1,000,000
 # reads, scale 1.0), from one ncu capture: profiles/dram_k_classify_dual_uneven-full_1M-reads.md
 DUAL_TRAFFIC_DEFAULT = 5_389_110_528 + 48_011_008

@@ -49,9 +49,12 @@ struct BatchDev {
   unsigned long long* n_cands;   // output cursor
   int* err;                      // OR of kErr* bits
   unsigned int* work;            // work-stealing cursor for the dual-strand warp tier
-  uint32_t* ovf0;                // reads handed to the general warp tier
+  uint32_t* ovf0;                // reads handed to the second dual-strand tier
   unsigned int* n_ovf0;
-  unsigned int* work1;           // cursor over ovf0
+  unsigned int* work0b;          // cursor over ovf0
+  uint32_t* ovf0b;               // reads handed to the general warp tier
+  unsigned int* n_ovf0b;
+  unsigned int* work1;           // cursor over ovf0b
   uint32_t* ovf1;                // reads handed to the block tier
   unsigned int* n_ovf1;
   unsigned int* work2;           // cursor over ovf1

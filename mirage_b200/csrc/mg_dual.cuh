@@ -18,19 +18,21 @@
 
 namespace mg {
 
-constexpr int kDualE = 64;               // postings per strand
-constexpr int kDualTab = 64;             // occurrence table entries per strand (>= distinct refs)
-
-// Per-warp shared memory of the dual path; [half] = strand.
-struct alignas(16) DualSmem {  // 16-byte aligned: the table clear stores 16 bytes a lane
-  uint32_t a[2][3][kDualE];     // gathered postings (ref, pos, found | seed << 8 | table entry << 16);
+// Per-warp shared memory of the dual path for up to Cap postings per strand (64 or 128; the kept
+// postings, at most 64, are tracked in 64-bit masks); [half] = strand. The occurrence table has
+// Cap entries, at least the distinct references of Cap postings.
+template <int Cap>
+struct alignas(16) DualSmemT {  // 16-byte aligned: the table clear stores 16 bytes a lane
+  static_assert(Cap == 64 || Cap == 128, "postings per strand");
+  uint32_t a[2][3][Cap];          // gathered postings (ref, pos, found | seed << 8 | table entry << 16);
                                 // from the rank sort on: kept postings sorted (ref, pos, seed)
-  uint32_t c[2][3][kDualE];     // kept postings, compacted (ref, pos, seed); at the end the run
+  uint32_t c[2][3][Cap];          // kept postings, compacted (ref, pos, seed); at the end the run
                                 // records' refID, first-seed position and last-seed end
-  uint32_t t[2][2][kDualTab];   // occurrence table (ref key, found mask, then occMax); from the
+  uint32_t t[2][2][Cap];          // occurrence table (ref key, found mask, then occMax); from the
                                 // diagonal runs on: the records' seed indices and segmax
   uint8_t q[2][kLeanQ];         // strand bases: forward, reverse complement
 };
+using DualSmem = DualSmemT<64>;  // the first dual tier, over every read
 
 __device__ __forceinline__ unsigned long long upto64(int i) {  // bits 0..i
   return i >= 63 ? ~0ull : ((2ull << i) - 1ull);
@@ -45,7 +47,8 @@ __device__ __forceinline__ uint32_t half_bits(uint32_t ballot, int sh) { return 
 // Both strands of one read (bases already in S.q). Warp-uniform return: kStrandOk, or
 // kStrandOverflow when either strand does not fit. Each lane receives its half's strand result:
 // *n_out run records (step 5) in S.c[half][0..2] and S.t[half][0], in ascending refID.
-__device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_t* n_out) {
+template <int Cap>
+__device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, uint32_t* n_out) {
   const unsigned FULL = 0xffffffffu;
   const uint32_t EMPTY = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15, sh = half * 16;
@@ -77,13 +80,13 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
       fnd = cnt > 0 || h == ix.empty_hash;
     }
     fb |= half_bits(__ballot_sync(FULL, fnd), sh) << (16 * s);
-    uint32_t x = cnt > (uint32_t)kDualE ? (uint32_t)kDualE + 1 : cnt;
+    uint32_t x = cnt > (uint32_t)Cap ? (uint32_t)Cap + 1 : cnt;
     for (int o = 1; o < 16; o <<= 1) {
       const uint32_t y = __shfl_up_sync(FULL, x, o, 16);
       if (hl >= o) x += y;
     }
     const uint32_t Tn = T + __shfl_sync(FULL, x, 15, 16);
-    if (__any_sync(FULL, Tn > (uint32_t)kDualE)) return kStrandOverflow;
+    if (__any_sync(FULL, Tn > (uint32_t)Cap)) return kStrandOverflow;
     const uint32_t f = __popc(fb & ((1u << j) - 1u));
     const uint32_t e = T + x - cnt;
     for (uint32_t t = 0; t < cnt; t++) {
@@ -98,20 +101,22 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
   if (!__any_sync(FULL, alive)) return kStrandOk;
   // 2. occurrence filter (Analyser.cpp:2057-2115): per reference, the found indices where it
   //    occurs (a table keyed by refID); the longest run of consecutive ones is its occMax
-  static_assert(kDualTab == 64, "the table clear below covers 64 entries with 16 lanes");
-  reinterpret_cast<uint4*>(tkey)[hl] = make_uint4(EMPTY, EMPTY, EMPTY, EMPTY);
-  reinterpret_cast<uint4*>(tval)[hl] = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+  for (int u = 0; u < Cap / 64; u++) {  // 16 lanes, 4 entries each per pass
+    reinterpret_cast<uint4*>(tkey)[hl + 16 * u] = make_uint4(EMPTY, EMPTY, EMPTY, EMPTY);
+    reinterpret_cast<uint4*>(tval)[hl + 16 * u] = make_uint4(0u, 0u, 0u, 0u);
+  }
   __syncwarp();
   const int nslw = (int)__reduce_max_sync(FULL, (T + 15) / 16);  // posting blocks, warp-uniform
   for (int s = 0; s < nslw; s++) {
     const uint32_t i = hl + 16 * s;
     if (i < T) {
       const uint32_t ref = e_ref[i];
-      uint32_t x = (ref * 2654435761u) >> 26;  // 64 entries
+      uint32_t x = (ref * 2654435761u) >> (Cap == 64 ? 26 : 25);  // Cap entries
       for (;;) {
         const uint32_t old = atomicCAS(&tkey[x], EMPTY, ref);
         if (old == EMPTY || old == ref) break;
-        x = (x + 1) & (kDualTab - 1);
+        x = (x + 1) & (Cap - 1);
       }
       const uint32_t fj = e_fj[i];
       atomicOr(&tval[x], 1u << (fj & 0xFFu));
@@ -120,7 +125,7 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
   }
   __syncwarp();
   int hs = 0;
-  for (int x = hl; x < kDualTab; x += 16)
+  for (int x = hl; x < Cap; x += 16)
     if (tkey[x] != EMPTY) {
       const int o = longest_run(tval[x]);
       tval[x] = (uint32_t)o;
@@ -152,6 +157,7 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
     T2 += __popc(kb);
   }
   __syncwarp();
+  if (Cap > 64 && __any_sync(FULL, T2 > 64u)) return kStrandOverflow;  // the masks below hold 64
   // 3. rank sort of the kept postings by (ref, pos, seed); the keys are distinct
   uint32_t* s_ref = S.a[half][0];
   uint32_t* s_pos = S.a[half][1];
@@ -246,7 +252,8 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmem& S, uint32_
 // The read's run records (forward strand first) go to its staging slots, or to the arena when
 // there are more than kSlots, and the read is marked kReadUnscored for k_finish_dual; a read
 // without records is final here (no candidate).
-__device__ bool process_read_dual(const DevIndex& ix, const BatchDev& b, uint32_t r, DualSmem& S,
+template <int Cap>
+__device__ bool process_read_dual(const DevIndex& ix, const BatchDev& b, uint32_t r, DualSmemT<Cap>& S,
                                   const uint8_t* comp, mg_candidate* stage, mg_candidate* arena, uint64_t arena_cap,
                                   unsigned long long* arena_n, int* errw) {
   const unsigned FULL = 0xffffffffu;

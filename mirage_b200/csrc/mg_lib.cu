@@ -276,7 +276,36 @@ __global__ void __launch_bounds__(kFinThreads) k_finish_dual(DevIndex ix, BatchD
   }
 }
 
-// General warp tier over the dual tier's leftovers; its own leftovers go to the block tier.
+// Second dual-strand tier over the first one's leftovers: room for 128 postings per strand (at
+// most 64 of them kept); the reads it takes leave run records for k_finish_dual like the first
+// tier's, its own leftovers go to the general warp tier. 4 warps per block (35 KB of shared memory).
+constexpr int kW2Warps = 4;
+__global__ void __launch_bounds__(kW2Warps * 32) k_classify_dual_list(DevIndex ix, BatchDev b, StageDev sd) {
+  __shared__ DualSmemT<128> sm[kW2Warps];
+  __shared__ uint8_t comp[256];
+  for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  DualSmemT<128>& S = sm[w];
+  const uint32_t n = *b.n_ovf0;
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(b.work0b, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= n) break;
+    const uint32_t r = b.ovf0[item];
+    if (!process_read_dual(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+      if (lane == 0) {
+        unsigned at = atomicAdd(b.n_ovf0b, 1u);
+        b.ovf0b[at] = r;
+        b.reads[r] = mg_read_result{};  // not kReadUnscored: a later tier writes this read
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// General warp tier over the dual tiers' leftovers; its own leftovers go to the block tier.
 __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp_list(DevIndex ix, BatchDev b, StageDev sd) {
   __shared__ WarpSmem sm[kW1Warps];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -291,13 +320,13 @@ __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp_list(DevIndex i
   ws.cb[0] = S.cb[0];
   ws.cb[1] = S.cb[1];
   const Caps caps{kW1Q, kW1Seeds, kW1E, kW1C};
-  const uint32_t n = *b.n_ovf0;
+  const uint32_t n = *b.n_ovf0b;
   for (;;) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(b.work1, 1u);
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= n) break;
-    const uint32_t r = b.ovf0[item];
+    const uint32_t r = b.ovf0b[item];
     if (!process_read<32>(ix, b, r, ws, caps, &S.red, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
       if (lane == 0) {
         unsigned at = atomicAdd(b.n_ovf1, 1u);
@@ -814,7 +843,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
   }
   if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
       w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
-      w.ovf.alloc(3 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+      w.ovf.alloc(4 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
@@ -822,7 +851,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 }
 
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
-// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1
+// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovf0b | 60 work0b
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
                         bool plain, unsigned long long* chain, const ChainSync* cs) {
@@ -844,7 +873,10 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   b.work3 = (unsigned*)(ctr + 36);
   b.n_ovf0 = (unsigned*)(ctr + 48);
   b.work1 = (unsigned*)(ctr + 52);
+  b.n_ovf0b = (unsigned*)(ctr + 56);
+  b.work0b = (unsigned*)(ctr + 60);
   b.ovf0 = w.ovf.as<uint32_t>();
+  b.ovf0b = w.ovf.as<uint32_t>() + 3 * (n + 4);
   b.ovf1 = w.ovf.as<uint32_t>() + n + 4;
   b.ovf2 = w.ovf.as<uint32_t>() + 2 * (n + 4);
   StageDev sd;
@@ -892,7 +924,8 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       int per_sm1 = 0;
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_classify_dual, kW1Warps * 32, 0);
       k_classify_dual<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
-      // the reads the dual tier handed on go through the other tiers on the side stream, beside
+      k_classify_dual_list<<<(unsigned)sms, kW2Warps * 32, 0, st>>>(ix->dix, b, sd);
+      // the reads the dual tiers handed on go through the other tiers on the side stream, beside
       // the dual tier's finishing pass (different reads, disjoint slots; arena space by atomics)
       CU(cudaEventRecord(w.fork, st));
       CU(cudaStreamWaitEvent(w.side, w.fork, 0));

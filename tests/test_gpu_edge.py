@@ -133,6 +133,45 @@ def test_many_candidates_grow_staging_arena(tmp_path, form):
     assert (r.reads["n_fwd"] + r.reads["n_rc"]).sum() >= 24 * 5000
 
 
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_strands_of_65_to_128_postings(tmp_path, form):
+    """Reads whose forward strand gathers 72 postings, 40 of them kept: five copies of the
+    reference the reads come from (kept: full diagonal runs) and eight decoy references holding
+    every other seed window of each read (never kept: their found indices alternate, so their
+    longest run is 1). Such strands exceed the first dual-strand tier's 64 postings and fit the
+    second one's 128 (with at most 64 kept); the results equal the oracle."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(29)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 20000)]
+    k, step, hlen, L = 31, 15, 17, 150
+    starts = np.arange(100) * 200
+    seqs = [core[s:s + L].tobytes() for s in starts]
+    ns = (L - k + step - 1) // step
+    decoys = []
+    for _ in range(8):
+        parts = []
+        for s in starts:
+            for j in range(0, ns, 2):
+                parts.append(core[s + j * step:s + j * step + hlen])
+                parts.append(acgt[rng.integers(0, 4, 20)])
+        decoys.append(np.concatenate(parts))
+    refs = [core] * 5 + decoys
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))], k=k)
+    path = tmp_path / "decoys.mhm"
+    image.tofile(path)
+    gix = M.Index(image, k=k)
+    oix = O.Index(str(path), k=k)
+    hashes = [O.lib().mgo_hash28(q[j * step:j * step + hlen], hlen) for q in seqs for j in range(ns)]
+    per_read = gix.bucket_sizes(np.array(hashes, np.uint32)).astype(np.int64).reshape(len(seqs), ns).sum(1)
+    assert (per_read > 64).all() and (per_read <= 128).all(), per_read
+    r = check_against_oracle(gix, oix, seqs, form)
+    assert (r.reads["n_fwd"] >= 5).all()
+
+
 def _tile(data, offs, times):
     n, nb = len(offs) - 1, int(offs[-1])
     o = np.concatenate([offs[:-1].astype(np.uint64) + np.uint64(k * nb) for k in range(times)] +
