@@ -50,7 +50,7 @@ N_READS = 1_000_000
 LAUNCHES_PER_BATCH = 9
 # DRAM bytes (read + write) of one k_classify_dual launch on the default workload (1,000,000
 # reads, scale 1.0), from one ncu capture: profiles/dram_k_classify_dual_uneven-full_1M-reads.md
-DUAL_TRAFFIC_DEFAULT = 5_389_110_528 + 48_011_008
+DUAL_TRAFFIC_DEFAULT = 5_389_143_040 + 49_829_632
 
 
 def log(*a):
