@@ -144,17 +144,6 @@ __global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix,
   }
 }
 
-// Finishing pass of the dual-strand tier, one thread per read it left kReadUnscored. The read's
-// run records (forward strand first, each strand in ascending refID; see process_read_dual) name
-// the run ends of the references whose longest run is M. Per record the head and tail walks
-// (head_walk, tail_walk) on the strand's bases, read from the batch: forward in upper case, the
-// reverse complement backwards through the complement table; the tail four bytes at a time while
-// the window has four left. Per reference the runs that scored
-// (T >= k) give the sums and the query coverage; a reference with such a run is a candidate:
-// Score, percentage and relative score (MatrixCPU.cpp:18-214, MatrixResult.cpp:21-29) replace its
-// records, compacted in place. Then the strand merge and top group as write_read_result_s
-// (Analyser.cpp:592-611, 388). One thread per read keeps every lane busy where the warp-per-read
-// kernel would run this one lane per run end.
 // Four bytes p..p+3, all readable, as one little-endian word: the aligned word holding p and,
 // only when p is not 4-aligned, the next aligned word (which holds p+3), so nothing outside
 // p..p+3's words is read.
@@ -173,106 +162,170 @@ __device__ __forceinline__ uint32_t upper4(uint32_t w) {
 
 constexpr int kFinThreads = 256;
 constexpr int kCovStride = kLeanQ / 32 + 1;  // coverage words per thread; odd, so no bank conflicts
+constexpr int kFinRecCap = 128;              // run records a warp walks together per 32 reads
 
+// The head and tail walks of one run record x (head_walk, tail_walk) on the strand's bases, read
+// from the batch (raw, L bytes): forward in upper case, the reverse complement backwards through
+// the complement table; the tail four bytes at a time while the window has four left. Returns the
+// run's query start << 16 | its extended length T, or 0 when T < k.
+__device__ __forceinline__ uint32_t walk_record(const DevIndex& ix, const uint8_t* comp, const uint8_t* raw, uint32_t L,
+                                                int strand, const mg_candidate& x, uint32_t k, uint32_t step) {
+  auto qb = [&](uint32_t p) -> uint8_t { return strand ? comp[raw[L - 1 - p]] : upper_dev(raw[p]); };
+  const uint8_t* rs = ix.bases + ix.ref_off[x.ref];
+  const uint32_t rlen = ix.ref_len[x.ref];
+  const uint32_t sr = __float_as_uint(x.rel), lr = __float_as_uint(x.score), jj = __float_as_uint(x.pct);
+  const uint32_t sq = (jj & 0xFFu) * step, lq = (jj >> 8) * step + step;
+  uint32_t tail = 0;
+  if (lq < L && lr < rlen) {
+    const uint32_t lim = min(min(rlen - lr, k), L - lq);
+    while (tail + 4 <= lim) {
+      uint32_t wq;
+      if (strand) {
+        const uint32_t w = load4(raw + (L - 4 - (lq + tail)));
+        wq = (uint32_t)comp[w >> 24] | ((uint32_t)comp[(w >> 16) & 0xFFu] << 8) |
+             ((uint32_t)comp[(w >> 8) & 0xFFu] << 16) | ((uint32_t)comp[w & 0xFFu] << 24);
+      } else {
+        wq = upper4(load4(raw + lq + tail));
+      }
+      if (wq ^ load4(rs + lr + tail)) break;
+      tail += 4;
+    }
+    while (tail < lim && qb(lq + tail) == rs[lr + tail]) tail++;
+  }
+  uint32_t head = 0;
+  const uint32_t hsz = min(sr, k);
+  if (sq != 0 && hsz != 0) {
+    const uint32_t jb = min(sq - 1, hsz - 1);
+    while (head < jb && qb(sq - 1 - head) == rs[sr - head]) head++;
+  }
+  const uint32_t tot = tail + head + (lq - sq);
+  return tot >= k ? ((sq - head) << 16) | tot : 0u;
+}
+
+// Finishing pass of the dual-strand tiers over the reads they left kReadUnscored, a warp per 32
+// consecutive reads. A read's run records (forward strand first, each strand in ascending refID;
+// see process_read_dual) name the run ends of the references whose longest run is M. The warp
+// walks its reads' records one per lane (walk_record), so that reads with many records or long
+// walks do not hold the other lanes; then each read's lane groups its records by reference: the
+// runs that scored (T >= k) give the sums and the query coverage, and a reference with such a run
+// is a candidate whose Score, percentage and relative score (MatrixCPU.cpp:18-214,
+// MatrixResult.cpp:21-29) replace its records, compacted in place; then the strand merge and top
+// group as write_read_result_s (Analyser.cpp:592-611, 388).
 __global__ void __launch_bounds__(kFinThreads) k_finish_dual(DevIndex ix, BatchDev b, StageDev sd) {
+  const unsigned FULL = 0xffffffffu;
   __shared__ uint8_t comp[256];
   __shared__ uint32_t covs[kFinThreads * kCovStride];
+  __shared__ uint32_t walks[kFinThreads / 32][kFinRecCap];
   for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   uint32_t* cov = covs + threadIdx.x * kCovStride;
+  uint32_t* zw = walks[threadIdx.x >> 5];
   const uint32_t k = (uint32_t)ix.k, step = (uint32_t)ix.step;
-  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < b.n; r += (uint64_t)gridDim.x * blockDim.x) {
-    mg_read_result rr = b.reads[r];
-    if (rr.strand != kReadUnscored) continue;
-    const uint64_t o0 = b.offs[r];
-    const uint32_t L = (uint32_t)(b.offs[r + 1] - o0);
-    const uint8_t* raw = b.bases + o0;
-    const uint32_t n0 = rr.n_fwd, nrec = n0 + rr.n_rc;
-    const bool big = nrec > (uint32_t)kSlots;
-    mg_candidate* rec = big ? sd.arena + rr.cand_off : sd.stage + r * kSlots;
-    const uint32_t nw = (L + 31) / 32;
-    int err = 0;
-    float hi[2] = {-1.0f, -1.0f};
-    uint32_t nc[2] = {0, 0}, out = 0;
-    for (int strand = 0; strand < 2; strand++) {
-      auto qb = [&](uint32_t x) -> uint8_t { return strand ? comp[raw[L - 1 - x]] : upper_dev(raw[x]); };
-      const uint32_t end = strand ? nrec : n0;
-      for (uint32_t g = strand ? n0 : 0; g < end;) {
-        const uint32_t ref = rec[g].ref;
-        const uint8_t* rs = ix.bases + ix.ref_off[ref];
-        const uint32_t rlen = ix.ref_len[ref];
-        uint32_t sumc = 0, sumr = 0, nsc = 0, e = g;
-        for (; e < end && rec[e].ref == ref; e++) {
-          const mg_candidate x = rec[e];
-          const uint32_t sr = __float_as_uint(x.rel), lr = __float_as_uint(x.score), jj = __float_as_uint(x.pct);
-          const uint32_t sq = (jj & 0xFFu) * step, lq = (jj >> 8) * step + step;
-          uint32_t tail = 0;  // tail_walk
-          if (lq < L && lr < rlen) {
-            const uint32_t lim = min(min(rlen - lr, k), L - lq);
-            while (tail + 4 <= lim) {  // four bytes at a time while all four are in the window
-              uint32_t wq;
-              if (strand) {
-                const uint32_t w = load4(raw + (L - 4 - (lq + tail)));
-                wq = (uint32_t)comp[w >> 24] | ((uint32_t)comp[(w >> 16) & 0xFFu] << 8) |
-                     ((uint32_t)comp[(w >> 8) & 0xFFu] << 16) | ((uint32_t)comp[w & 0xFFu] << 24);
-              } else {
-                wq = upper4(load4(raw + lq + tail));
-              }
-              const uint32_t x = wq ^ load4(rs + lr + tail);
-              if (x) break;
-              tail += 4;
-            }
-            while (tail < lim && qb(lq + tail) == rs[lr + tail]) tail++;
-          }
-          uint32_t head = 0;  // head_walk
-          const uint32_t hsz = min(sr, k);
-          if (sq != 0 && hsz != 0) {
-            const uint32_t jb = min(sq - 1, hsz - 1);
-            while (head < jb && qb(sq - 1 - head) == rs[sr - head]) head++;
-          }
-          const uint32_t tot = tail + head + (lq - sq);
-          if (tot < k) continue;
-          if (nsc++ == 0)
-            for (uint32_t wd = 0; wd < nw; wd++) cov[wd] = 0;
-          sumc += tot;
-          sumr += tot * (tot + 1) / 2;
-          const uint32_t a = sq - head, bnd = a + tot;
-          for (uint32_t wd = a >> 5; wd <= (bnd - 1) >> 5; wd++) {
-            const uint32_t w0 = wd * 32;
-            const uint32_t lo = a > w0 ? a : w0, up = bnd < w0 + 32 ? bnd : w0 + 32;
-            const uint32_t n = up - lo;
-            cov[wd] |= (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0);
-          }
+  // a warp takes 32 consecutive reads, one per lane
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < b.n;
+       base += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = base + lane;
+    mg_read_result rr{};
+    bool mine = false;
+    if (r < b.n) {
+      rr = b.reads[r];
+      mine = rr.strand == kReadUnscored;
+    }
+    const uint32_t n0 = mine ? rr.n_fwd : 0u, nrec = mine ? n0 + rr.n_rc : 0u;
+    uint64_t o0 = 0;
+    uint32_t L = 0;
+    mg_candidate* rec = nullptr;
+    if (mine) {
+      o0 = b.offs[r];
+      L = (uint32_t)(b.offs[r + 1] - o0);
+      rec = nrec > (uint32_t)kSlots ? sd.arena + rr.cand_off : sd.stage + r * kSlots;
+    }
+    uint32_t incl = nrec;  // the warp's records, read by read
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t excl = incl - nrec, total = __shfl_sync(FULL, incl, 31);
+    if (total == 0) continue;
+    // the walks, one record per lane across the warp's reads (up to kFinRecCap records; beyond
+    // that each lane walks its own read's records below)
+    const bool together = total <= (uint32_t)kFinRecCap;
+    if (together) {
+      for (uint32_t gb = 0; gb < total; gb += 32) {
+        const uint32_t g = gb + lane;
+        uint32_t o = 0;  // the lane whose read holds record g: the lanes before it end at or below g
+        for (int bit = 16; bit > 0; bit >>= 1)
+          if (__shfl_sync(FULL, incl, o + bit - 1) <= g) o += bit;
+        const uint32_t oe = __shfl_sync(FULL, excl, o), on0 = __shfl_sync(FULL, n0, o);
+        const uint32_t oL = __shfl_sync(FULL, L, o);
+        const uint64_t oo = __shfl_sync(FULL, (unsigned long long)o0, o);
+        const mg_candidate* orec = (const mg_candidate*)__shfl_sync(FULL, (unsigned long long)rec, o);
+        if (g < total) {
+          const uint32_t i = g - oe;
+          zw[g] = walk_record(ix, comp, b.bases + oo, oL, i >= on0 ? 1 : 0, orec[i], k, step);
         }
-        if (nsc) {
-          uint32_t hits = 0;
-          for (uint32_t wd = 0; wd < nw; wd++) hits += __popc(cov[wd]);
-          float sc, pc;
-          final_score(sumr, sumc, hits, L, &sc, &pc);
-          const float rl = relative_score_tab(ix, L, rlen, sc, &err);
-          rec[out++] = mg_candidate{ref, rl, sc, pc};  // out <= g: this group's records are read
-          nc[strand]++;
-          hi[strand] = fmaxf(hi[strand], rl);
-        }
-        g = e;
       }
+      __syncwarp();
     }
-    const uint32_t tot = nc[0] + nc[1];
-    mg_candidate* fin = rec;
-    if (big && tot <= (uint32_t)kSlots) {  // k_scatter takes up to kSlots candidates from the slots
-      fin = sd.stage + r * kSlots;
-      for (uint32_t c = 0; c < tot; c++) fin[c] = rec[c];
+    if (mine) {
+      const uint8_t* raw = b.bases + o0;
+      const bool big = nrec > (uint32_t)kSlots;
+      const uint32_t nw = (L + 31) / 32;
+      int err = 0;
+      float hi[2] = {-1.0f, -1.0f};
+      uint32_t nc[2] = {0, 0}, out = 0;
+      for (int strand = 0; strand < 2; strand++) {
+        const uint32_t end = strand ? nrec : n0;
+        for (uint32_t g = strand ? n0 : 0; g < end;) {
+          const uint32_t ref = rec[g].ref;
+          uint32_t sumc = 0, sumr = 0, nsc = 0, e = g;
+          for (; e < end && rec[e].ref == ref; e++) {
+            const uint32_t z = together ? zw[excl + e] : walk_record(ix, comp, raw, L, strand, rec[e], k, step);
+            if (!z) continue;
+            const uint32_t tot = z & 0xFFFFu, a = z >> 16, bnd = a + tot;
+            if (nsc++ == 0)
+              for (uint32_t wd = 0; wd < nw; wd++) cov[wd] = 0;
+            sumc += tot;
+            sumr += tot * (tot + 1) / 2;
+            for (uint32_t wd = a >> 5; wd <= (bnd - 1) >> 5; wd++) {
+              const uint32_t w0 = wd * 32;
+              const uint32_t lo = a > w0 ? a : w0, up = bnd < w0 + 32 ? bnd : w0 + 32;
+              const uint32_t n = up - lo;
+              cov[wd] |= (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0);
+            }
+          }
+          if (nsc) {
+            uint32_t hits = 0;
+            for (uint32_t wd = 0; wd < nw; wd++) hits += __popc(cov[wd]);
+            float sc, pc;
+            final_score(sumr, sumc, hits, L, &sc, &pc);
+            const float rl = relative_score_tab(ix, L, ix.ref_len[ref], sc, &err);
+            rec[out++] = mg_candidate{ref, rl, sc, pc};  // out <= g: this group's records are read
+            nc[strand]++;
+            hi[strand] = fmaxf(hi[strand], rl);
+          }
+          g = e;
+        }
+      }
+      const uint32_t tot = nc[0] + nc[1];
+      mg_candidate* fin = rec;
+      if (big && tot <= (uint32_t)kSlots) {  // k_scatter takes up to kSlots candidates from the slots
+        fin = sd.stage + r * kSlots;
+        for (uint32_t c = 0; c < tot; c++) fin[c] = rec[c];
+      }
+      const int ch = hi[0] < hi[1] ? 1 : 0;  // Analyser.cpp:601
+      const uint32_t nch = nc[ch];
+      const float hch = hi[ch];
+      const mg_candidate* cc = fin + (ch ? nc[0] : 0);
+      uint32_t top = 0;
+      for (uint32_t i = 0; i < nch; i++) top += cc[i].rel == hch;
+      rr = mg_read_result{hch, tot > (uint32_t)kSlots ? rr.cand_off : 0u, (uint16_t)nc[0], (uint16_t)nc[1],
+                          (uint8_t)ch, (uint8_t)((nch > 0 && hch != 0.0f) ? 1 : 0), (uint16_t)top};  // Analyser.cpp:388
+      b.reads[r] = rr;
+      if (err) atomicOr(b.err, err);
     }
-    const int ch = hi[0] < hi[1] ? 1 : 0;  // Analyser.cpp:601
-    const uint32_t nch = nc[ch];
-    const float hch = hi[ch];
-    const mg_candidate* cc = fin + (ch ? nc[0] : 0);
-    uint32_t top = 0;
-    for (uint32_t i = 0; i < nch; i++) top += cc[i].rel == hch;
-    rr = mg_read_result{hch, tot > (uint32_t)kSlots ? rr.cand_off : 0u, (uint16_t)nc[0], (uint16_t)nc[1], (uint8_t)ch,
-                        (uint8_t)((nch > 0 && hch != 0.0f) ? 1 : 0), (uint16_t)top};  // reported: Analyser.cpp:388
-    b.reads[r] = rr;
-    if (err) atomicOr(b.err, err);
+    __syncwarp();  // zw is the next reads' before any lane leaves these
   }
 }
 
