@@ -133,6 +133,29 @@ def test_many_candidates_grow_staging_arena(tmp_path, form):
     assert (r.reads["n_fwd"] + r.reads["n_rc"]).sum() >= 24 * 5000
 
 
+def test_warps_with_more_run_records_than_they_walk_together(tmp_path):
+    """Every read matches 7 identical references: 56 postings per strand, all kept, and 7 run
+    records per read, so a warp's 32 reads hold 224 records, more than the finishing pass walks
+    one per lane (128); each read's lane then walks its own. The results equal the oracle."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(31)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 20000)]
+    refs = [core] * 7 + [acgt[rng.integers(0, 4, 20000)] for _ in range(2)]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))])
+    path = tmp_path / "seven.mhm"
+    image.tofile(path)
+    gix = M.Index(image)
+    oix = O.Index(str(path))
+    starts = rng.integers(0, 20000 - 150, 512)
+    seqs = [core[s:s + 150].tobytes() for s in starts]
+    r = check_against_oracle(gix, oix, seqs)
+    assert (r.reads["n_fwd"] + r.reads["n_rc"] >= 7).all()
+
+
 @pytest.mark.parametrize("form", ["batched", "plain"])
 def test_strands_of_65_to_128_postings(tmp_path, form):
     """Reads whose forward strand gathers 72 postings, 40 of them kept: five copies of the
