@@ -169,6 +169,32 @@ def algorithmic_bytes(ix, reads, n_cands: int, k: int = 31) -> dict:
             "ref_windows": 64 * n_cands, "results": 16 * (len(lens) + n_cands), "seeds": n_seeds}
 
 
+def h2d_link_gbs(h_bases, d_bases):
+    """Bandwidth of a plain copy of the pinned host bases to the device (5 copies after 2 warm-up
+    copies, CUDA events), the bound the end-to-end figure is read against; None if it fails."""
+    try:
+        import torch
+
+        with torch.cuda.device(d_bases.device):
+            dst = torch.empty_like(d_bases)
+            stream = torch.cuda.current_stream(d_bases.device)
+            for _ in range(2):
+                dst.copy_(h_bases, non_blocking=True)
+            torch.cuda.synchronize()
+            c0 = torch.cuda.Event(enable_timing=True)
+            c1 = torch.cuda.Event(enable_timing=True)
+            c0.record(stream)
+            for _ in range(5):
+                dst.copy_(h_bases, non_blocking=True)
+            c1.record(stream)
+            torch.cuda.synchronize()
+            gbs = 5 * h_bases.numel() / (c0.elapsed_time(c1) / 1000) / 1e9
+            del dst
+            return gbs
+    except Exception:  # a diagnostic: never fails the benchmark
+        return None
+
+
 def mhm_word(img: np.ndarray) -> int:
     """The .mhm word width (4 or 8): the 32-bit field 12 bytes after the 73-byte magic text."""
     return int.from_bytes(img[85:89].tobytes(), "little")
@@ -430,6 +456,7 @@ def main():
         e2e = world * n / e2e_s
     h2d = n_bases + 8 * (n + 1)
     d2h = 16 * n + 16 * n_c + 64
+    link_gbs = h2d_link_gbs(h_bases, d_bases)
 
     # plain form (one block per read), same e2e measurement
     for _ in range(2):
@@ -499,7 +526,10 @@ def main():
                            "l2": "inputs larger than L2 (index + reads), no flush",
                            "parallelism": f"replicas x{world}, reads sharded"},
                 "e2e": {"value": e2e, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "ms_per_step": 1000 * e2e_s, "host_buffers": "pinned"},
+                        "ms_per_step": 1000 * e2e_s, "host_buffers": "pinned",
+                        "link_h2d_gbs": link_gbs,
+                        "link_what": "plain pinned-host-to-device copy of the step's bases on this machine, "
+                                     "outside the timed regions"},
                 "plain": {"value": plain, "unit": "reads/s", "ms_per_step": 1000 * plain_s,
                           "what": "mg_score_batch e2e (one block per read, one launch per batch)"},
                 "batched_over_plain_e2e": e2e / plain,
