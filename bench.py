@@ -504,6 +504,8 @@ def main():
                 "traffic_what": "DRAM bytes per k_classify_dual launch, one ncu capture of this workload "
                                 "(profiles/dram_k_classify_dual_uneven-full_1M-reads.md)" if default_run else None,
                 "gather_peak": gather, "frac_of_gather": achieved / gather,
+                # the probe's own bytes (directory sectors + posting sectors) over the same time
+                "probe_frac_of_gather": (ab["directory"] + ab["postings"]) / (warp_ms / 1000) / 1e9 / gather,
                 "gather_peak_what": "random 32-byte sector gathers, 8 lanes per sector, over a 4 GiB buffer "
                                     "(mg_gather_bandwidth), measured in this run",
                 "kernel": "classification: k_classify_dual + k_finish_dual, beside them the general, block "
