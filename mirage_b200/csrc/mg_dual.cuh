@@ -10,9 +10,10 @@
 //   rank sort          over the kept postings only, compacted first (usually about one per seed)
 // so the serial work per strand follows the kept postings, not all of them, and the two strands
 // run side by side. The kernel stops at the diagonal runs: the run ends of the references that can
-// become candidates leave as 16-byte records, and k_finish_dual (mg_lib.cu) walks, covers and
-// scores them one thread per read, work whose one-lane-per-run form would leave most lanes idle. Nothing is indexed dynamically in registers; per-posting state lives in
-// shared memory, whose regions are reused from step to step.
+// become candidates leave as 16-byte records, and k_finish_dual (mg_lib.cu) walks them one record
+// per lane and covers and scores them one read per lane, work whose one-lane-per-run form here
+// would leave most lanes idle. Nothing is indexed dynamically in registers; per-posting state
+// lives in shared memory, whose regions are reused from step to step.
 #pragma once
 #include "mg_lean.cuh"
 
@@ -221,7 +222,7 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
   // 5. one record per run end of a kept reference whose longest run is M (the references that can
   //    become candidates): refID, reference position of the run's first seed, reference end of its
   //    last seed, the two seed indices. The head/tail walks, coverage and scores of these runs are
-  //    k_finish_dual's (one thread per read). The records go to shared memory regions free by now.
+  //    k_finish_dual's. The records go to shared memory regions free by now.
   uint32_t* r_ref = S.c[half][0];
   uint32_t* r_sr = S.c[half][1];
   uint32_t* r_lr = S.c[half][2];

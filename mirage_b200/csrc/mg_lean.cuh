@@ -9,8 +9,8 @@
 //   sort (ref, pos, q)     rank sort of the kept postings (keys are distinct)
 //   diagonal runs          run starts as a bit mask; run length = i - last start + 1
 //                          (Analyser.cpp:2337-2490)
-//   scoring                sums and coverage one lane per candidate reference (MatrixCPU.cpp:18-208);
-//                          the scores from them one thread per read in k_finish_dual (mg_lib.cu)
+//   scoring                head/tail walks, coverage and scores in k_finish_dual (mg_lib.cu), from
+//                          one record per run end (MatrixCPU.cpp:18-214)
 #pragma once
 #include "mg_kernels.cuh"
 
