@@ -48,9 +48,12 @@ N_READS = 1_000_000
 # kernels one batched call launches: dual-strand tier, second dual-strand tier (its leftovers),
 # the finishing pass, general warp tier, block tier, global tier, candidate count, scan, scatter
 LAUNCHES_PER_BATCH = 9
-# DRAM bytes (read + write) of one k_classify_dual launch on the default workload (1,000,000
-# reads, scale 1.0), from one ncu capture: profiles/dram_k_classify_dual_uneven-full_1M-reads.md
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_classify_dual launch on the
+# default workload (1,000,000 reads, scale 1.0): a constant from one ncu capture of this kernel,
+# not a measurement of this run
 DUAL_TRAFFIC_DEFAULT = 5_389_143_040 + 49_829_632
+DUAL_TRAFFIC_WHAT = ("DRAM bytes per k_classify_dual launch: a constant from one ncu capture of the kernel on "
+                     "this workload (dram__bytes_read.sum + dram__bytes_write.sum), not measured in this run")
 
 
 def log(*a):
@@ -133,35 +136,47 @@ def hash28_windows_2d(seqs: np.ndarray) -> np.ndarray:
     return (((x >> 28) ^ x) & 0x0FFFFFFF).astype(np.uint32)
 
 
+_COMP = np.zeros(256, np.uint8)
+for _a, _b in zip(b"ACGTN", b"TGCAN"):
+    _COMP[_a] = _b
+
+
+def seed_hashes(data: np.ndarray, offs: np.ndarray, k: int = 31, chunk_seeds: int = 1 << 21):
+    """The hashes of every seed of both strands (Analyser.cpp:1453-1478: seeds at p = 0, step,
+    2 step, ... while p < L - k; the reverse complement read from the forward bytes), yielded in
+    chunks of about chunk_seeds."""
+    step, h = k // 2, k - k // 2 + 1
+    offs = offs.astype(np.int64)
+    lens = np.diff(offs)
+    ns = np.where(lens > k, (lens - k + step - 1) // step, 0)
+    cum = np.concatenate([[0], np.cumsum(ns)])
+    i0, n = 0, len(lens)
+    while i0 < n:
+        i1 = int(np.searchsorted(cum, cum[i0] + chunk_seeds, side="right"))
+        i1 = min(n, max(i1, i0 + 1))
+        cnt = ns[i0:i1]
+        rid = np.repeat(np.arange(i0, i1), cnt)
+        j = np.arange(int(cnt.sum())) - np.repeat(cum[i0:i1] - cum[i0], cnt)
+        p = j * step
+        o, L = offs[rid], lens[rid]
+        yield hash28_windows_2d(data[(o + p)[:, None] + np.arange(h)[None, :]])
+        yield hash28_windows_2d(_COMP[data[(o + L - 1 - p)[:, None] - np.arange(h)[None, :]]])
+        i0 = i1
+
+
 def algorithmic_bytes(ix, reads, n_cands: int, k: int = 31) -> dict:
     """Bytes the path must move per batch (each term one access a minimal implementation
     cannot avoid): the read bytes; per seed of both strands one 32-byte directory sector and the
     32-byte sectors holding its postings (8 bytes each); per scored candidate two 32-byte
     reference windows (head and tail of at least one run); 16 bytes of result per read and per
     candidate."""
-    step, h = k // 2, k - k // 2 + 1
     lens = reads.lengths().astype(np.int64)
-    data = reads.data
-    comp = np.zeros(256, np.uint8)
-    for a, b in zip(b"ACGTN", b"TGCAN"):
-        comp[a] = b
-    seed_bytes = 0
     post_bytes = 0
     n_seeds = 0
-    for L in np.unique(lens):
-        if L <= k:
-            continue
-        idx = np.flatnonzero(lens == L)
-        starts = reads.offs[idx].astype(np.int64)
-        mat = data[starts[:, None] + np.arange(L)[None, :]]
-        for strand in (0, 1):
-            m = mat if strand == 0 else comp[mat[:, ::-1]]
-            ns = (L - k + step - 1) // step
-            for j in range(ns):
-                hs = hash28_windows_2d(m[:, j * step : j * step + h])
-                cnt = ix.bucket_sizes(hs).astype(np.int64)
-                n_seeds += len(hs)
-                post_bytes += int((((cnt * 8) + 31) // 32 * 32).sum())
+    for hs in seed_hashes(reads.data, reads.offs, k):
+        cnt = ix.bucket_sizes(hs).astype(np.int64)
+        n_seeds += len(hs)
+        post_bytes += int((((cnt * 8) + 31) // 32 * 32).sum())
     seed_bytes = 32 * n_seeds
     read_bytes = int(lens.sum())
     total = read_bytes + seed_bytes + post_bytes + 64 * n_cands + 16 * len(lens) + 16 * n_cands
@@ -200,18 +215,58 @@ def mhm_word(img: np.ndarray) -> int:
     return int.from_bytes(img[85:89].tobytes(), "little")
 
 
-def make_workload(scale: float, n_reads: int, rank: int):
-    from mirage_b200 import synth
+def load_synth():
+    """The seeded workload generator (mirage_b200/synth.py, numpy only), loaded from its file so
+    that the reference arm's process never imports the mirage_b200 package or its library."""
+    import importlib.util
 
-    # one reference set (seed SEED) for every rank, one read set per rank
-    refs, reads, _ = synth.workload("uneven_fast", scale, seed=SEED, n_reads=n_reads, reads_seed=SEED + 1 + rank)
+    if "mg_synth" not in sys.modules:
+        spec = importlib.util.spec_from_file_location("mg_synth", os.path.join(ROOT, "mirage_b200", "synth.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["mg_synth"] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules["mg_synth"]
+
+
+# The workloads (one per configuration quoted for this path); `uneven` is the default line.
+WORKLOADS = {
+    "uneven": {"synth": "uneven_fast", "reads": 1_000_000, "cpu_sample": 100_000,
+               "what": "uneven: {refs} refs {bp} bp log-normal (median 50 kb, sigma 0.8, GC 0.3-0.7), {n} reads "
+                       "75-300 bp per GPU (0.5% subs, 0.1% indels, 20% unrelated)"},
+    "long": {"synth": "long_fast", "reads": 100_000, "cpu_sample": 2_000,
+             "what": "long: {refs} refs {bp} bp log-normal (the uneven references), {n} reads per GPU, log-normal "
+                     "length median 5 kb clipped to 1-20 kb, 3% subs + 2% indels, 10% chimeras"},
+    "plain": {"synth": "plain", "reads": 11_000, "cpu_sample": 11_000,
+              "what": "plain: {refs} refs x 5,000 bp uniform, {n} reads of 150 bp per GPU (1% subs, 1 in 11 unrelated)"},
+    "large": {"synth": "repeats", "reads": 10_000_000, "cpu_sample": 50_000,
+              "what": "large: {refs} refs {bp} bp log-normal (median 80 kb) with 5% shared repeat segments, {n} reads "
+                      "of 250 bp per GPU (1% subs)"},
+}
+
+
+def make_workload(scale: float, n_reads: int, rank: int, workload: str = "uneven"):
+    synth = load_synth()
+    w = WORKLOADS[workload]
+    if w["synth"] in ("uneven_fast", "long_fast"):
+        # one reference set (seed SEED) for every rank, one read set per rank
+        refs, reads, _ = synth.workload(w["synth"], scale, seed=SEED, n_reads=n_reads, reads_seed=SEED + 1 + rank)
+    else:
+        refs, reads, _ = synth.workload(w["synth"], scale, seed=SEED + rank, n_reads=n_reads)
     return refs, reads
 
 
-def cpu_baseline(img: np.ndarray, reads, word: int, sample: int) -> dict:
-    """The reference CPU path (oracle harness) on a bounded sample, all host threads; the CPU
-    restatement when the reference harness is not built."""
+def workload_text(workload: str, refs, n: int) -> str:
+    return WORKLOADS[workload]["what"].format(refs=len(refs), bp=int(refs.offs[-1]), n=n)
+
+
+def cpu_baseline_and_parity(img: np.ndarray, reads, word: int, sample: int, gpu_reads: np.ndarray,
+                            gpu_cands: np.ndarray) -> tuple[dict, dict | None]:
+    """The reference CPU path (oracle harness) on the first `sample` reads of the batch with all
+    host threads, one strand per job (per-read semantics); its dump of those reads is then
+    compared bit for bit with the GPU's results for the same reads (from the e2e run). The CPU
+    restatement is timed instead when the reference harness is not built (no parity then)."""
     from oracle import oracle as O
+    from oracle import parity as P
 
     threads = os.cpu_count() or 1
     sub = reads.subset(min(sample, len(reads)))
@@ -221,66 +276,84 @@ def cpu_baseline(img: np.ndarray, reads, word: int, sample: int) -> dict:
         harness = O.HARNESS if word == 4 else O.HARNESS + "64"
         if os.path.exists(harness):
             fa = os.path.join(tmp, "reads.fasta")
+            dump = os.path.join(tmp, "ref.dump")
             sub.write_fasta(fa)
-            js = json.loads(O.run_harness(mhm, fa, job=1, threads=threads, time_only=True, word=word))
-            return {"value": len(sub) / js["hot_s"], "unit": "reads/s", "cores": threads, "kind": "reference",
-                    "sample": f"{len(sub)} reads of the same workload; reference TPrepareGPUAnalysis + "
-                              f"CPUGetHighestScore + strand merge (index load excluded)"}
+            js = json.loads(O.run_harness(mhm, fa, out=dump, job=1, threads=threads, word=word))
+            cpu = {"value": len(sub) / js["hot_s"], "unit": "reads/s", "cores": threads, "kind": "reference",
+                   "sample": f"the first {len(sub)} reads of the batch; reference TPrepareGPUAnalysis + "
+                             f"CPUGetHighestScore + strand merge, one strand per job on {threads} threads "
+                             f"(index load excluded)"}
+            t = time.perf_counter()
+            want = P.canon_from_dump(O.parse_dump(dump))
+            got = P.canon_from_arrays(gpu_reads, gpu_cands, len(sub))
+            par = P.count_mismatches(want, got)
+            par["examples"] = P.diff(want, got, limit=3)
+            par["against"] = ("reference CPU path (oracle/_ref harness: TPrepareGPUAnalysis -> CPUGetHighestScore "
+                              "-> strand merge, one strand per job) on the same reads and the same index")
+            par["fields"] = ("per strand: scored candidates (refID, Score, percentageMatch, relative score bits) "
+                             "and HighestScore bits; per read: kept strand, merged HighestScore bits, top group")
+            par["gpu_results_from"] = "the last timed e2e step (mg_classify, host buffers)"
+            par["compare_s"] = time.perf_counter() - t
+            return cpu, par
         oix = O.Index(mhm)
         oix.count(sub.data[: int(sub.offs[min(1000, len(sub))])], sub.offs[: min(1000, len(sub)) + 1], threads)
         t = time.perf_counter()
         oix.count(sub.data, sub.offs, threads)
         dt = time.perf_counter() - t
         return {"value": len(sub) / dt, "unit": "reads/s", "cores": threads, "kind": "port",
-                "sample": f"{len(sub)} reads of the same workload through the CPU restatement"}
+                "sample": f"{len(sub)} reads of the same workload through the CPU restatement"}, None
 
 
 def run_reference_arm(args, rank: int, world: int) -> None:
-    """--impl reference: the reference's CPU implementation on host cores."""
+    """--impl reference: the reference's own CPU path on the host cores, on this arm's workload
+    (the full batch per step). The index is built by the reference's own stock program from the
+    references' FASTA, and the timed region is the reference harness's hot path under the stock
+    program's thread scheme; this process never loads the mirage_b200 library."""
     if rank != 0:
         return
-    import mirage_b200 as M
     from oracle import oracle as O
 
-    refs, reads = make_workload(args.scale, args.reads, 0)
-    img = M.build_image(refs.data, refs.offs, refs.headers, k=31)
-    word = mhm_word(img)
-    threads = os.cpu_count() or 1
-    per_step = args.ref_sample
+    refs, reads = make_workload(args.scale, args.reads, 0, args.workload)
+    total_bp = int(refs.offs[-1])
+    word = 8 if total_bp > 150_000_000 else 4  # the 32-bit layout stops at 4 GB of .mhm
     harness = O.HARNESS if word == 4 else O.HARNESS + "64"
-    kind = "reference" if os.path.exists(harness) else "port"
-    times = []
+    threads = os.cpu_count() or 1
+    line = {"impl": "reference", "metric": "reads/s", "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic"}
+    if not os.path.exists(harness) or not os.path.exists(O.MIRAGE_REF + ("64" if word == 8 else "")):
+        line["unavailable"] = "the reference CPU path (oracle/_ref) is not built on this machine"
+        print(json.dumps(line), flush=True)
+        return
+    n = len(reads)
     with tempfile.TemporaryDirectory(prefix="mg_ref_") as tmp:
-        mhm = os.path.join(tmp, "index.mhm")
-        img.tofile(mhm)
-        del img
-        if kind == "reference":
-            fa = os.path.join(tmp, "reads.fasta")
-            reads.subset(per_step).write_fasta(fa)
-            out = subprocess.run([harness, "--mhm", mhm, "--reads", fa, "--job", "1", "--threads", str(threads),
-                                  "--time", "--repeat", str(args.warmup + args.steps)],
-                                 capture_output=True, text=True, check=True).stderr
-            for line in out.splitlines():
-                if line.startswith('{"rep"'):
-                    times.append(json.loads(line)["hot_s"])
-        else:
-            oix = O.Index(mhm)
-            sub = reads.subset(per_step)
-            for _ in range(args.warmup + args.steps):
-                t = time.perf_counter()
-                oix.count(sub.data, sub.offs, threads)
-                times.append(time.perf_counter() - t)
-    timed = times[args.warmup:]
+        rf = os.path.join(tmp, "refs.fasta")
+        fa = os.path.join(tmp, "reads.fasta")
+        refs.write_fasta(rf)
+        reads.write_fasta(fa)
+        t0 = time.time()
+        mhm = O.build_mhm_with_reference(rf, os.path.join(tmp, "build"), word=word)
+        t_build = time.time() - t0
+        reps = O.run_harness(mhm, fa, word=word, scheme="stock", time_only=True, repeat=args.warmup + args.steps,
+                             all_lines=True)
+    timed = [r["hot_s"] for r in reps[args.warmup:]]
     ms = 1000 * float(np.mean(timed))
-    value = per_step / (ms / 1000)
-    line = {"impl": "reference", "metric": "reads/s", "value": value, "unit": "reads/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": "uneven: 5000 refs ~344 Mbp log-normal, 1M reads 75-300 bp per GPU",
-                       "sample_reads_per_step": per_step},
-            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": kind,
-                             "sample": f"{per_step} reads of the workload per step"},
-            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    value = n / (ms / 1000)
+    r0 = reps[-1]
+    line.update({
+        "value": value, "ms_per_step": ms,
+        "config": {"workload": workload_text(args.workload, refs, n), "k": 31, "mhm_word": word,
+                   "reads_per_step": n},
+        "scheme": {"prepare_workers": r0["threads"], "strands_per_job": r0["job"],
+                   "what": "the stock program's scheduling: numCores x 4 TPrepareGPUAnalysis workers over jobs of "
+                           "2 x max(1, reads / (numCores x 40 + 1)) strands (Analyser.cpp:3500-3503, 3712-3724), "
+                           "then MatrixCPU::CPUGetHighestScore's own tasks, strand merge and top group; the whole "
+                           "batch as one block"},
+        "index": {"built_by": "the reference's stock program (oracle/_ref/mirage_ref%s) from the references' FASTA"
+                              % ("64" if word == 8 else ""), "build_s": t_build, "load_s": r0["load_s"]},
+        "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "reference",
+                         "sample": f"all {n} reads of the batch per step (index build and load excluded)"},
+        "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     print(json.dumps(line), flush=True)
 
 
@@ -335,14 +408,23 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mirage", choices=["mirage", "reference"])
+    ap.add_argument("--workload", default="uneven", choices=sorted(WORKLOADS),
+                    help="uneven (default): 5,000 refs, 1M reads of 75-300 bp; long: the same refs, 100k reads "
+                         "of 1-20 kb; plain: 200 x 5 kb refs, 11k reads of 150 bp; large: 20,000 refs ~2 Gbp "
+                         "with shared repeats, 10M reads of 250 bp")
     ap.add_argument("--scale", type=float, default=1.0, help="shrink the reference set (tests)")
-    ap.add_argument("--reads", type=int, default=N_READS, help="reads per GPU per step")
-    ap.add_argument("--cpu-sample", type=int, default=100_000)
-    ap.add_argument("--ref-sample", type=int, default=100_000)
+    ap.add_argument("--reads", type=int, default=None, help="reads per GPU per step (default: the workload's)")
+    ap.add_argument("--cpu-sample", type=int, default=None, help="reads of the CPU baseline and parity sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--served-seconds", type=float, default=3.0, help="seconds per served-form load level (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.reads is None:
+        args.reads = WORKLOADS[args.workload]["reads"]
+    if args.cpu_sample is None:
+        args.cpu_sample = WORKLOADS[args.workload]["cpu_sample"]
+    if args.workload != "uneven":
+        args.served_seconds = 0.0  # the served form is measured on the uneven workload (its request shape)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -364,7 +446,7 @@ def main():
     import mirage_b200 as M
 
     t0 = time.time()
-    refs, reads = make_workload(args.scale, args.reads, rank)
+    refs, reads = make_workload(args.scale, args.reads, rank, args.workload)
     t_gen = time.time() - t0
     t0 = time.time()
     img = M.build_image(refs.data, refs.offs, refs.headers, k=31, device=local)  # same bytes as the host build
@@ -497,12 +579,11 @@ def main():
         warp_ms = float(np.mean(step_ms)) - kernel_ms[4] / args.steps
         achieved = ab["bytes"] / (warp_ms / 1000) / 1e9
         gather = M.gather_bandwidth(local, 4 << 30)
-        default_run = args.scale == 1.0 and args.reads == N_READS
+        default_run = args.workload == "uneven" and args.scale == 1.0 and args.reads == N_READS
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm or 6650.0, "unit": "GB/s",
                 "frac": achieved / (hbm or 6650.0),
                 "traffic": DUAL_TRAFFIC_DEFAULT if default_run else None,
-                "traffic_what": "DRAM bytes per k_classify_dual launch, one ncu capture of this workload "
-                                "(profiles/dram_k_classify_dual_uneven-full_1M-reads.md)" if default_run else None,
+                "traffic_what": DUAL_TRAFFIC_WHAT if default_run else None,
                 "gather_peak": gather, "frac_of_gather": achieved / gather,
                 # the probe's own bytes (directory sectors + posting sectors) over the same time
                 "probe_frac_of_gather": (ab["directory"] + ab["postings"]) / (warp_ms / 1000) / 1e9 / gather,
@@ -513,17 +594,17 @@ def main():
                 "kernel_ms": warp_ms,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": ab}
-        cpu = None
+        cpu, parity = None, None
         if not args.no_cpu_baseline and world == 1:
             try:
-                cpu = cpu_baseline(img, reads, word, args.cpu_sample)
+                cpu, parity = cpu_baseline_and_parity(img, reads, word, args.cpu_sample, h_reads.numpy(),
+                                                      h_cands.numpy()[: 16 * n_c])
             except Exception as e:  # reported, not fatal
                 cpu = {"value": None, "error": str(e)[:200]}
         line = {"metric": "reads/s", "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-                "config": {"workload": f"uneven: {len(refs)} refs {int(refs.offs[-1])} bp log-normal, "
-                                       f"{n} reads 75-300 bp per GPU (0.5% subs, 0.1% indels, 20% unrelated)",
+                "config": {"workload": workload_text(args.workload, refs, n),
                            "index_bytes": len(img), "mhm_word": word, "k": 31,
                            "l2": "inputs larger than L2 (index + reads), no flush",
                            "parallelism": f"replicas x{world}, reads sharded"},
@@ -544,7 +625,7 @@ def main():
                                        "block_tier": kernel_ms[2] / args.steps,
                                        "global_tier": kernel_ms[3] / args.steps,
                                        "compaction": kernel_ms[4] / args.steps},
-                "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk.summary(),
                 "gpu_launches": args.steps * LAUNCHES_PER_BATCH,
                 "setup_s": {"generate": t_gen, "index_build_device": t_build, "open": t_open}}
         print(json.dumps(line), flush=True)

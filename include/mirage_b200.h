@@ -103,6 +103,7 @@ typedef struct {
   uint64_t device_bytes;   /* HBM held by the index */
   int32_t k, word;         /* k and the .mhm word width (4 or 8) */
   double load_seconds, upload_seconds;
+  int32_t probe_slots;     /* 1 while the hash-slot table is built (mg_set_probe_slots) */
 } mg_index_info;
 
 /* Replaces Hashmap::ReadHashmapFile (Hashmap.cpp:329) for one file: parses the .mhm, decodes
@@ -134,6 +135,14 @@ int mg_eval_logf(mg_index* ix, const float* x, float* out, uint64_t n);
  * beside the finishing pass. mg_bucket_sizes returns the number of postings stored under each
  * of n 28-bit hashes (the index directory, read on the device). */
 int mg_set_timing(mg_index* ix, int on);
+/* Layout of the seed probe (no counterpart in the reference, whose probe is an unordered_map
+ * find, Analyser.cpp:1483-1519). With on = 1 the index holds a hash-slot table: 64 bytes per
+ * 28-bit hash (17.2 GB of HBM) with the bucket's posting count, its first posting's offset and its
+ * first 7 postings, so the dual-strand tiers read most seeds' postings from one 64-byte block;
+ * with on = 0 they read the 4-byte directory and then the postings. mg_open builds the table for
+ * indexes of at least 2^25 postings. Results are the same either way. Waits for the device to be
+ * idle; MG_ERR_BUSY while a server (mg_server_create) is attached to the index. */
+int mg_set_probe_slots(mg_index* ix, int on);
 /* Diagnostic (no counterpart in the reference): the roofline of the lookup path. Times 2^26
  * gathers of whole 32-byte sectors (8 lanes per sector) at pseudo-random positions of a device
  * buffer of the largest power of two <= buffer_bytes (use several times the L2 size) on
@@ -198,7 +207,10 @@ int mg_classify_device_sync(mg_index* ix, void* stream, uint64_t* n_cands);
  * bytes bases[q_off[s]..q_off[s+1]), already normalised), candidates cand_ref[c_off[s] ..
  * c_off[s+1]) with runs run[r_off[c] .. r_off[c+1]) given as 4 uint32 (Start.Reference,
  * Start.Query, Last.Reference, Last.Query). Outputs Score, percentageMatch and relative score
- * per candidate (score -2 and rel -1 for unscored candidates) and HighestScore per strand. */
+ * per candidate (score -2 and rel -1 for unscored candidates) and HighestScore per strand.
+ * A candidate reference beyond the index, or a walked run (Start.Query <= Last.Query) whose
+ * Last.Query exceeds its query length or whose Start.Reference lies beyond its reference, is
+ * refused with MG_ERR_INVAL before anything is copied to the device. */
 int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off,
                         const uint8_t* bases, const uint64_t* c_off, const uint32_t* cand_ref,
                         const uint64_t* r_off, const uint32_t* runs, float* score, float* pct,
@@ -210,11 +222,13 @@ int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off,
  * pointers on ix's device, plus a stream (NULL = the index's stream); it calls no cudaMalloc or
  * cudaFree. Its working memory is a fixed 4,849,920-byte array that the library holds on every
  * GPU that loads it, until exit; that caps a query strand at 2048 bases (longer ones: MG_ERR_LIMIT,
- * and their candidates are left unscored). The first call on each device looks up the array's
- * device address; make that first call before any stream capture. Every call on a device uses the
- * same array: calls whose GPU work overlapped would race on it, so the library serialises its
- * calls and each returns after its GPU work has ended. A candidate reference or run outside its
- * reference or query returns MG_ERR_INVAL. */
+ * and their candidates are left unscored). Every call, the first included, ends by waiting for
+ * its own GPU work on `stream` (it reads the array's error word back). The first call on each
+ * device also looks up the array's device address, a set-up step that has to come before any
+ * stream capture begins on that device. Every call on a device uses the same array: calls whose
+ * GPU work overlapped would race on it, so the library serialises the calls on each device
+ * (calls on different devices do not wait for each other). A candidate reference or run outside
+ * its reference or query returns MG_ERR_INVAL, as it does in mg_score_candidates. */
 int mg_score_candidates_noalloc(mg_index* ix, uint64_t n_strands, const uint64_t* d_q_off,
                                 const uint8_t* d_bases, const uint64_t* d_c_off,
                                 const uint32_t* d_cand_ref, const uint64_t* d_r_off,

@@ -24,7 +24,7 @@ ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LI
           -6: "MG_ERR_BADINPUT", -7: "MG_ERR_TIMEOUT", -8: "MG_ERR_INVAL", -9: "MG_ERR_BUSY"}
 
 EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
-           "mg_set_timing", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
+           "mg_set_timing", "mg_set_probe_slots", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
            "mg_build_image", "mg_build_image_device", "mg_parse_fasta_device", "mg_seqs_free", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_poll",
@@ -54,7 +54,7 @@ class _Result(C.Structure):
 class _Info(C.Structure):
     _fields_ = [("n_hashes", C.c_uint64), ("n_postings", C.c_uint64), ("n_refs", C.c_uint64),
                 ("ref_bases", C.c_uint64), ("device_bytes", C.c_uint64), ("k", C.c_int32), ("word", C.c_int32),
-                ("load_seconds", C.c_double), ("upload_seconds", C.c_double)]
+                ("load_seconds", C.c_double), ("upload_seconds", C.c_double), ("probe_slots", C.c_int32)]
 
 
 class _ServerConfig(C.Structure):
@@ -99,6 +99,7 @@ def lib() -> C.CDLL:
         L.mg_server_destroy.argtypes = [vp]
         L.mg_server_destroy.restype = None
         L.mg_set_timing.argtypes = [vp, i32]
+        L.mg_set_probe_slots.argtypes = [vp, i32]
         L.mg_gather_bandwidth.argtypes = [i32, u64, C.POINTER(C.c_double)]
         L.mg_last_kernel_times.argtypes = [vp, vp]
         L.mg_bucket_sizes.argtypes = [vp, vp, vp, u64]
@@ -289,6 +290,10 @@ class Index:
         L = lib()
         fn = L.mg_classify if form == "batched" else L.mg_score_batch
         return self._run(fn, "mg_classify" if form == "batched" else "mg_score_batch", bases, offsets, cand_cap)
+
+    def set_probe_slots(self, on: bool = True) -> None:
+        """Build (or drop) the hash-slot table the dual-strand tiers probe (mg_set_probe_slots)."""
+        _check(lib().mg_set_probe_slots(self.h, 1 if on else 0), "mg_set_probe_slots")
 
     def set_timing(self, on: bool = True) -> None:
         _check(lib().mg_set_timing(self.h, 1 if on else 0), "mg_set_timing")

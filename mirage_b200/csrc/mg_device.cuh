@@ -12,10 +12,19 @@ constexpr uint32_t kLogLoBits = 0x3F800000u;  // 1.0f
 constexpr uint32_t kLogHiBits = 0x49800000u;  // 2^20
 constexpr uint32_t kLogDomain = kLogHiBits - kLogLoBits;
 
+// Hash slots: one 64-byte slot per 28-bit hash, 64-byte aligned. Word 0 holds the bucket's
+// posting count, word 1 its first posting in post, words 2-15 its first kSlotPosts postings as
+// (refID, position) pairs: a seed whose bucket holds at most kSlotPosts postings gets all of them
+// from one 64-byte block instead of a directory sector and then a dependent posting sector.
+constexpr int kSlotPosts = 7;
+constexpr int kSlotVecs = 4;  // uint4 per slot
+
 // HBM-resident index (all pointers device memory).
 struct DevIndex {
   const uint32_t* dir;      // 2^28 + 1 bucket offsets into post (CSR over the 28-bit hash)
   const uint2* post;        // (refID, position) per posting, bucket order
+  const uint4* slots;       // 2^28 hash slots (kSlotVecs uint4 each), or nullptr: probes read dir
+                            // and post
   const uint8_t* bases;     // reference sequence block
   const uint64_t* ref_off;  // offset of each reference in bases
   const uint32_t* ref_len;

@@ -73,11 +73,24 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
   for (int s = 0; s < nsb; s++) {
     const uint32_t j = hl + 16 * s;
     uint32_t cnt = 0, o0 = 0;
+    uint4 v0 = make_uint4(0u, 0u, 0u, 0u), v1 = v0, v2 = v0, v3 = v0;  // the seed's hash slot
     bool fnd = false;
     if (j < ns) {
       const uint32_t h = hash28_dev(q + j * step, ix.hlen);
-      o0 = __ldg(ix.dir + h);
-      cnt = __ldg(ix.dir + h + 1) - o0;
+      if (ix.slots) {
+        const uint4* sl = ix.slots + (size_t)h * kSlotVecs;
+        v0 = __ldg(sl);
+        v1 = __ldg(sl + 1);
+        cnt = v0.x;
+        o0 = v0.y;
+        if (cnt > 3) {  // postings 3-6 lie in the slot's second 32-byte sector
+          v2 = __ldg(sl + 2);
+          v3 = __ldg(sl + 3);
+        }
+      } else {
+        o0 = __ldg(ix.dir + h);
+        cnt = __ldg(ix.dir + h + 1) - o0;
+      }
       fnd = cnt > 0 || h == ix.empty_hash;
     }
     fb |= half_bits(__ballot_sync(FULL, fnd), sh) << (16 * s);
@@ -90,11 +103,30 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
     if (__any_sync(FULL, Tn > (uint32_t)Cap)) return kStrandOverflow;
     const uint32_t f = __popc(fb & ((1u << j) - 1u));
     const uint32_t e = T + x - cnt;
-    for (uint32_t t = 0; t < cnt; t++) {
+    const uint32_t fj = f | (j << 8);
+    uint32_t t0 = 0;
+    if (ix.slots) {
+      auto put = [&](uint32_t t, uint32_t ref, uint32_t pos) {
+        if (t < cnt) {
+          e_ref[e + t] = ref;
+          e_pos[e + t] = pos;
+          e_fj[e + t] = fj;
+        }
+      };
+      put(0, v0.z, v0.w);
+      put(1, v1.x, v1.y);
+      put(2, v1.z, v1.w);
+      put(3, v2.x, v2.y);
+      put(4, v2.z, v2.w);
+      put(5, v3.x, v3.y);
+      put(6, v3.z, v3.w);
+      t0 = kSlotPosts;
+    }
+    for (uint32_t t = t0; t < cnt; t++) {
       const uint2 p = __ldg(ix.post + o0 + t);
       e_ref[e + t] = p.x;
       e_pos[e + t] = p.y;
-      e_fj[e + t] = f | (j << 8);
+      e_fj[e + t] = fj;
     }
     T = Tn;
   }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -96,7 +97,7 @@ struct mg_index {
   int device = 0;
   mg::DevIndex dix{};
   mg::MhmIndex host;  // refs, headers, taxids kept; postings released after upload
-  mg::DevBuf dir, post, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals, log_den;
+  mg::DevBuf dir, post, slots, bases, ref_off, ref_len, logx_bitmap, logx_keys, logx_vals, log_den;
   mg::Workspace ws;   // workspace of the synchronous entry points
   cudaStream_t stream = nullptr;
   // chunked batched form: copy streams and per-chunk events (made on first use)
@@ -107,6 +108,7 @@ struct mg_index {
   mg::Workspace ws2;                     // scratch of the odd chunks
   bool chunk_made = false;
   std::mutex mu;
+  std::atomic<int> n_servers{0};  // mg_server objects attached to this index
   mg_index_info info{};
   uint64_t device_bytes = 0;
   // optional per-kernel timing of the last pipeline (events on the launching stream)

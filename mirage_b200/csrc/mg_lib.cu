@@ -637,6 +637,23 @@ __global__ void k_fill_dir64(const uint32_t* toc_hash, const uint64_t* toc_start
   for (uint64_t h = lo; h <= hi; h++) dir[h] = v;
 }
 
+// Hash slots from the directory and the postings: count, first posting and the first kSlotPosts
+// postings of every 28-bit hash (zeros beyond the bucket).
+__global__ void k_fill_slots(const uint32_t* dir, const uint2* post, uint4* slots) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t h = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; h < (1ull << 28); h += stride) {
+    const uint32_t o = dir[h], cnt = dir[h + 1] - o;
+    uint2 p[kSlotPosts];
+#pragma unroll
+    for (int t = 0; t < kSlotPosts; t++) p[t] = (uint32_t)t < cnt ? post[o + t] : make_uint2(0u, 0u);
+    uint4* sl = slots + h * kSlotVecs;
+    sl[0] = make_uint4(cnt, o, p[0].x, p[0].y);
+    sl[1] = make_uint4(p[1].x, p[1].y, p[2].x, p[2].y);
+    sl[2] = make_uint4(p[3].x, p[3].y, p[4].x, p[4].y);
+    sl[3] = make_uint4(p[5].x, p[5].y, p[6].x, p[6].y);
+  }
+}
+
 __global__ void k_log_probe(uint32_t lo_bits, uint32_t n, float* out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = log_dev_raw(__uint_as_float(lo_bits + i));
@@ -785,6 +802,28 @@ static int build_log_table(mg_index* ix) {
   return MG_OK;
 }
 
+// Hash slots (DevIndex::slots) are built at open for indexes of at least this many postings; the
+// table takes 2^28 x 64 bytes (17.2 GB) whatever the index size, which small indexes do not repay.
+constexpr uint64_t kSlotsFromPostings = 1ull << 25;
+
+static int set_probe_slots(mg_index* ix, bool on) {
+  if (!on) {
+    ix->slots.release();
+    ix->dix.slots = nullptr;
+    return MG_OK;
+  }
+  if (ix->dix.slots) return MG_OK;
+  if (ix->slots.alloc((1ull << 28) * kSlotVecs * sizeof(uint4)))
+    return set_error(MG_ERR_OOM, "device memory for the hash slots");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
+  k_fill_slots<<<(unsigned)sms * 8, 256, 0, ix->stream>>>(ix->dix.dir, ix->dix.post, ix->slots.as<uint4>());
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(ix->stream));
+  ix->dix.slots = ix->slots.as<uint4>();
+  return MG_OK;
+}
+
 // The HBM index from a .mhm image: the host parses the header and reference tables; the image
 // is copied to the device once and the bucket TOC and posting records are decoded there.
 static int upload_index_image(mg_index* ix, const uint8_t* image, uint64_t L, const MhmMeta& meta, int k) {
@@ -860,6 +899,10 @@ static int upload_index_image(mg_index* ix, const uint8_t* image, uint64_t L, co
   d.k = k;
   d.step = k / 2;
   d.hlen = k - k / 2 + 1;
+  if (total >= kSlotsFromPostings) {
+    const int rc = set_probe_slots(ix, true);
+    if (rc) return rc;
+  }
   return build_log_table(ix);
 }
 
@@ -1263,8 +1306,8 @@ int mg_open_image(const uint8_t* image, uint64_t len, int k, int device, mg_inde
 void mg_close(mg_index* ix) {
   if (!ix) return;
   cudaSetDevice(ix->device);
-  for (DevBuf* b : {&ix->dir, &ix->post, &ix->bases, &ix->ref_off, &ix->ref_len, &ix->logx_bitmap, &ix->logx_keys,
-                    &ix->logx_vals, &ix->log_den})
+  for (DevBuf* b : {&ix->dir, &ix->post, &ix->slots, &ix->bases, &ix->ref_off, &ix->ref_len, &ix->logx_bitmap,
+                    &ix->logx_keys, &ix->logx_vals, &ix->log_den})
     b->release();
   ix->ws.release();
   if (ix->stream) cudaStreamDestroy(ix->stream);
@@ -1288,6 +1331,8 @@ void mg_close(mg_index* ix) {
 int mg_index_get_info(const mg_index* ix, mg_index_info* info) {
   if (!ix || !info) return set_error(MG_ERR_INVAL, "null argument");
   *info = ix->info;
+  info->device_bytes = ix->device_bytes + ix->slots.n;
+  info->probe_slots = ix->dix.slots != nullptr;
   return MG_OK;
 }
 
@@ -1330,6 +1375,15 @@ int mg_inspect_image(const uint8_t* image, uint64_t len, int k, mg_index_info* i
   info->word = h.word;
   info->load_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return MG_OK;
+}
+
+int mg_set_probe_slots(mg_index* ix, int on) {
+  if (!ix) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  if (ix->n_servers.load() > 0) return set_error(MG_ERR_BUSY, "a server is attached to the index");
+  CU(cudaSetDevice(ix->device));
+  CU(cudaDeviceSynchronize());  // no kernel of an earlier call still reads the table
+  return set_probe_slots(ix, on != 0);
 }
 
 int mg_set_timing(mg_index* ix, int on) {
@@ -1514,6 +1568,17 @@ int mg_score_candidates(mg_index* ix, uint64_t n_strands, const uint64_t* q_off,
   std::vector<uint64_t> cs(nc);
   for (uint64_t s = 0; s < n_strands; s++)
     for (uint64_t c = c_off[s]; c < c_off[s + 1]; c++) cs[c] = s;
+  // a run the kernel walks (Start.Query <= Last.Query) must lie inside its query and reference:
+  // its coverage ends at Last.Query + tail <= L and its head walk starts at Start.Reference
+  for (uint64_t c = 0; c < nc; c++) {
+    const uint64_t L = q_off[cs[c] + 1] - q_off[cs[c]];
+    const uint32_t rlen = ix->host.ref_len[cand_ref[c]];
+    for (uint64_t r = r_off[c]; r < r_off[c + 1]; r++) {
+      const uint32_t sref = runs[4 * r], sq = runs[4 * r + 1], lq = runs[4 * r + 3];
+      if (sq <= lq && (lq > L || sref >= rlen))
+        return set_error(MG_ERR_INVAL, "a candidate run lies outside its reference or query");
+    }
+  }
   const uint64_t hw = (maxL + 31) / 32 + 1;
   DevBuf dq, db, dr, drun, dcs, dro, dsc, dpc, drl, dhit, derr;
   if (dq.alloc((n_strands + 1) * 8) || db.alloc(nb + 16) || dr.alloc(nc * 4 + 4) || drun.alloc(nr * 16 + 16) ||

@@ -116,7 +116,7 @@ __global__ void k_strand_highest(uint64_t n_strands, const uint64_t* c_off, cons
   highest[s] = h;
 }
 
-std::mutex g_na_mu;                         // serialises the calls of this process
+std::mutex g_na_mu[kNaMaxDevices];          // serialises the calls on each device (one array each)
 void* g_na_addr[kNaMaxDevices] = {};        // device address of the array, per device
 
 }  // namespace
@@ -137,7 +137,7 @@ extern "C" int mg_score_candidates_noalloc(mg_index* ix, uint64_t n_strands, con
   if (n_strands >= (1ull << 40)) return set_error(MG_ERR_LIMIT, "too many query strands");
   const int dev = ix->device;
   if (dev < 0 || dev >= kNaMaxDevices) return set_error(MG_ERR_LIMIT, "device ordinal beyond the supported range");
-  std::lock_guard<std::mutex> lk(g_na_mu);
+  std::lock_guard<std::mutex> lk(g_na_mu[dev]);
   int prev = -1;
   if (cudaGetDevice(&prev) != cudaSuccess) return set_error(MG_ERR_CUDA, "cudaGetDevice");
   if (prev != dev && cudaSetDevice(dev) != cudaSuccess) return set_error(MG_ERR_CUDA, "cudaSetDevice");

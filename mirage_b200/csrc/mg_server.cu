@@ -366,6 +366,7 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
     }
   }
   sv->th = std::thread(server_loop, sv);
+  ix->n_servers++;
   *out = sv;
   return MG_OK;
 }
@@ -464,6 +465,7 @@ void mg_server_destroy(mg_server* sv) {
   cudaSetDevice(sv->ix->device);
   for (auto& s : sv->slot) slot_free(s);
   if (sv->ring.base) cudaFreeHost(sv->ring.base);
+  sv->ix->n_servers--;
   delete sv;
 }
 

@@ -16,6 +16,8 @@ Workloads (``scale`` shrinks counts, never per-sequence shapes):
               (the benchmark's form: one reference set, one read set per GPU).
 * ``long``    the same references; 100,000 reads, log-normal length (median 5 kb, clipped to
               1-20 kb), 3% substitutions + 2% indels, 10% chimeras of two references.
+* ``long_fast`` the same shapes with a vectorised read generator and a separate read seed
+              (the benchmark's form of ``long``).
 * ``repeats`` 20,000 references, log-normal (median 80 kb, sigma 0.67), 5% of every reference
               overwritten by segments of 500-5,000 bp from a pool of 1,000 shared segments;
               10,000,000 reads of 250 bp with 1% substitutions.
@@ -128,10 +130,12 @@ def make_references(n_refs: int, lengths: np.ndarray, gc: np.ndarray, rng) -> Se
     return SeqSet(data, offs, [b"ref%d" % i for i in range(n_refs)])
 
 
-def _substitute(rng, seq: np.ndarray, rate: float) -> None:
+def _substitute(rng, seq: np.ndarray, rate: float, chunk: int = 1 << 26) -> None:
     if rate <= 0 or len(seq) == 0:
         return
-    m = np.flatnonzero(rng.random(len(seq)) < rate)
+    # uniform draws in chunks (the same stream as one draw of len(seq))
+    m = np.concatenate([np.flatnonzero(rng.random(min(chunk, len(seq) - a)) < rate) + a
+                        for a in range(0, len(seq), chunk)])
     if len(m):
         code = np.searchsorted(ACGT, seq[m])
         code = np.where(code < 4, code, 0)
@@ -206,10 +210,14 @@ def _fast_fixed_reads(refs: SeqSet, n_related: int, n_unrelated: int, L: int, rn
     r = ok[rng.integers(0, len(ok), size=n_related)]
     p = (rng.random(n_related) * (rlen[r] - L + 1)).astype(np.int64)
     start = refs.offs[r].astype(np.int64) + p
-    idx = start[:, None] + np.arange(L)[None, :]
-    rel = refs.data[idx]
+    rel = np.empty((n_related, L), np.uint8)
+    for c in range(0, n_related, 1 << 20):  # gathered in row blocks (no n x L index matrix)
+        rel[c : c + (1 << 20)] = refs.data[start[c : c + (1 << 20), None] + np.arange(L)[None, :]]
     flip = rng.random(n_related) < 0.5
-    rel[flip] = _COMP[rel[flip][:, ::-1]]
+    fi = np.flatnonzero(flip)
+    for c in range(0, len(fi), 1 << 20):
+        rows = fi[c : c + (1 << 20)]
+        rel[rows] = _COMP[rel[rows][:, ::-1]]
     flat = rel.reshape(-1)
     _substitute(rng, flat, sub)
     unrel = ACGT[rng.integers(0, 4, size=n_unrelated * L).astype(np.uint8)]
@@ -268,12 +276,79 @@ def _fast_variable_reads(refs: SeqSet, n_related: int, n_unrelated: int, lo: int
     return SeqSet(data, offs, [b"read%d" % i for i in range(n)]), truth
 
 
+def _fast_long_reads(refs: SeqSet, n: int, rng, sub: float, indel: float, chimera_frac: float,
+                     median: int = 5000, sigma: float = 0.8, lo: int = 1000, hi: int = 20000, chunk: int = 4096):
+    """Vectorised long reads: log-normal lengths clipped to [lo, hi]; a chimera fraction joins
+    two references at a uniform breakpoint; single-base indels at rate `indel` (half
+    insertions of a uniform base, half deletions), then substitutions at rate `sub` of the
+    read's bases, then the reverse complement of half the reads. Returns the reads and the
+    reference of each read's first part."""
+    lens = _lognormal_lengths(rng, n, median, sigma, lo=lo, hi=hi)
+    rlen = refs.lengths().astype(np.int64)
+    roffs = refs.offs.astype(np.int64)
+    truth = np.empty(n, np.int64)
+    out_offs = np.zeros(n + 1, np.uint64)
+    out_offs[1:] = np.cumsum(lens)
+    data = np.empty(int(out_offs[-1]), np.uint8)
+    for c0 in range(0, n, chunk):
+        c1 = min(n, c0 + chunk)
+        m = c1 - c0
+        L = lens[c0:c1]
+        W = int(L.max()) + int(4 * indel * L.max()) + 64  # source window: the read plus its deletions
+        chim = rng.random(m) < chimera_frac
+        cut = np.where(chim, (rng.random(m) * (L - 1)).astype(np.int64) + 1, L)  # bases from the first part
+        need_a = np.where(chim, cut + 64, W)
+        ra = np.empty(m, np.int64)
+        rb = np.empty(m, np.int64)
+        for dst, need in ((ra, need_a), (rb, np.where(chim, W, 0))):
+            pick = rng.integers(0, len(refs), size=m)
+            bad = rlen[pick] < need + 2
+            while bad.any():
+                pick[bad] = rng.integers(0, len(refs), size=int(bad.sum()))
+                bad = rlen[pick] < need + 2
+            dst[:] = pick
+        pa = (rng.random(m) * (rlen[ra] - need_a - 1)).astype(np.int64)
+        pb = (rng.random(m) * np.maximum(rlen[rb] - W - 1, 1)).astype(np.int64)
+        q = np.arange(W)[None, :]
+        src = np.where(q < cut[:, None], roffs[ra][:, None] + pa[:, None] + q,
+                       roffs[rb][:, None] + pb[:, None] + (q - cut[:, None]))
+        srcb = refs.data[src]
+        # indel events per output position: insertion or deletion, each at rate indel / 2
+        ev = rng.random((m, W))
+        valid = q < L[:, None]
+        ins = (ev < indel / 2) & valid
+        dele = (ev >= indel / 2) & (ev < indel) & valid
+        # source index of output j: j - insertions before j + deletions up to and including j
+        sidx = np.clip(q - (np.cumsum(ins, axis=1) - ins) + np.cumsum(dele, axis=1), 0, W - 1)
+        read = np.take_along_axis(srcb, sidx, axis=1)
+        read[ins] = ACGT[rng.integers(0, 4, size=int(ins.sum())).astype(np.uint8)]
+        flat = read[valid]
+        _substitute(rng, flat, sub)
+        starts = out_offs[c0:c1].astype(np.int64) - int(out_offs[c0])
+        for i in np.flatnonzero(rng.random(m) < 0.5):  # reverse complement of half the reads
+            a, b = int(starts[i]), int(starts[i] + L[i])
+            flat[a:b] = _COMP[flat[a:b][::-1]]
+        data[int(out_offs[c0]) : int(out_offs[c1])] = flat
+        truth[c0:c1] = ra
+    return SeqSet(data, out_offs, [b"read%d" % i for i in range(n)]), truth
+
+
 def workload(name: str, scale: float = 1.0, seed: int = 1, n_reads: int | None = None,
              reads_seed: int | None = None, refs: SeqSet | None = None):
     """Return (references, reads, truth) for a named workload. With reads_seed the reads come
     from their own generator (so several read sets can share one reference set, which `refs`
     may pass in already generated)."""
     rng = np.random.default_rng(seed)
+    if name == "long_fast":
+        n_refs = max(4, int(round(5000 * scale)))
+        if refs is None:
+            total = 344e6 * n_refs / 5000
+            lens = _lognormal_lengths(rng, n_refs, 50_000, 0.8, lo=1000, total=total, tol=0.1)
+            refs = make_references(n_refs, lens, rng.uniform(0.3, 0.7, size=n_refs), rng)
+        rr = np.random.default_rng(reads_seed if reads_seed is not None else seed + 1_000_003)
+        nr = n_reads if n_reads is not None else int(round(100_000 * scale))
+        reads, truth = _fast_long_reads(refs, nr, rr, 0.03, 0.02, 0.1)
+        return refs, reads, truth
     if name == "uneven_fast":
         n_refs = max(4, int(round(5000 * scale)))
         if refs is None:

@@ -227,9 +227,16 @@ def compare(a: Result, b: Result, max_report: int = 10) -> list[str]:
 
 def run_harness(mhm: str, reads_fasta: str, out: str | None = None, job: int = 1,
                 threads: int = 1, logdir: str | None = None, time_only: bool = False,
-                limit: int | None = None, word: int = 4) -> str:
-    """Run the reference harness (oracle/_ref/mg_ref_harness); returns its timing JSON line."""
+                limit: int | None = None, word: int = 4, scheme: str | None = None, repeat: int = 1,
+                all_lines: bool = False):
+    """Run the reference harness (oracle/_ref/mg_ref_harness); returns its last timing JSON
+    line (all of them, one per repetition, as dicts when all_lines). scheme "stock": the stock
+    program's worker count and job size instead of job / threads (see ref_harness.cpp)."""
     cmd = [HARNESS if word == 4 else HARNESS + "64", "--mhm", mhm, "--reads", reads_fasta, "--job", str(job), "--threads", str(threads)]
+    if scheme:
+        cmd += ["--scheme", scheme]
+    if repeat > 1:
+        cmd += ["--repeat", str(repeat)]
     if out:
         cmd += ["--out", out]
     if logdir:
@@ -242,6 +249,10 @@ def run_harness(mhm: str, reads_fasta: str, out: str | None = None, job: int = 1
     if p.returncode != 0:
         raise RuntimeError(f"harness failed: {p.stderr[-2000:]}")
     lines = [l for l in p.stderr.splitlines() if l.startswith("{")]
+    if all_lines:
+        import json
+
+        return [json.loads(l) for l in lines]
     return lines[-1] if lines else ""
 
 

@@ -26,9 +26,15 @@
 // program's grouping (N strands per job, forward/reverse pairs adjacent) so the size of that
 // defect can be measured.
 //
+// `--scheme stock` times the stock program's own scheduling instead: numCores x 4 prepare
+// workers (Analyser.cpp:3500-3503) over jobs of numQIDs_PerThread strands, where
+// numQIDs_PerThread = 2 * max(1, n_reads / (numCores x 40 + 1)), made even (Analyser.cpp:
+// 3712-3724), with the sample taken as one batch; numCores = std::thread::hardware_concurrency.
+// Its candidate lists carry the stale-flag defect above, so it is a timing mode, not a dump mode.
+//
 // Usage:
 //   mg_ref_harness --mhm X.mhm --reads R.fasta [--out dump.txt] [--job N] [--threads T]
-//                  [--logdir DIR] [--time] [--limit NREADS]
+//                  [--scheme stock] [--logdir DIR] [--time] [--limit NREADS]
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -120,6 +126,7 @@ struct Opts {
   int k = 31;
   bool first_only = true;
   bool parse_only = false;
+  bool stock = false;
 };
 
 static void usage() {
@@ -149,6 +156,11 @@ int main(int argc, char** argv) {
     else if (a == "--k") o.k = std::stoi(next());
     else if (a == "--all-groups") o.first_only = false;
     else if (a == "--parse-only") o.parse_only = true;
+    else if (a == "--scheme") {
+      const std::string v = next();
+      if (v == "stock") o.stock = true;
+      else if (v != "job") usage();
+    }
     else usage();
   }
   if (o.mhm.empty() || o.reads.empty()) usage();
@@ -231,6 +243,15 @@ int main(int argc, char** argv) {
     qids.push_back((SEQ_ID_t)(i + n_total));
   }
   size_t nq = qids.size();
+  if (o.stock) {
+    // Analyser.cpp:3500-3503 (workers) and 3712-3724 (strands per job)
+    const size_t cores = std::max(1u, std::thread::hardware_concurrency());
+    const size_t total_prepare = cores * 40 + 1;
+    size_t per = std::max<size_t>(1, n_reads / total_prepare) * 2;
+    per -= per % 2;
+    o.job = per;
+    o.threads = (int)(cores * 4);
+  }
 
   // --time --repeat R: the hot path R times over the same reads (the index stays loaded);
   // one JSON line per repetition.

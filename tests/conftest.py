@@ -15,8 +15,16 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); run with -m gpu")
 
 
-def golden_cases():
-    return sorted(d for d in os.listdir(GOLDEN) if os.path.exists(os.path.join(GOLDEN, d, "meta.json")))
+def golden_cases(large: bool = False):
+    """Golden fixture names; large cases (full-scale indexes, GPU tests only) when asked."""
+    out = []
+    for d in sorted(os.listdir(GOLDEN)):
+        meta = os.path.join(GOLDEN, d, "meta.json")
+        if os.path.exists(meta):
+            with open(meta) as f:
+                if large or not json.load(f).get("large"):
+                    out.append(d)
+    return out
 
 
 def _fasta_bytes(seqset) -> bytes:
@@ -52,8 +60,9 @@ class GoldenCase:
         if self._image is None:
             import mirage_b200 as M
 
+            # large cases are built by the device build (same bytes as the host writer)
             self._image = M.build_image(self.refs.data, self.refs.offs, self.refs.headers, k=self.meta["k"],
-                                        word=self.meta["word"])
+                                        word=self.meta["word"], device=0 if self.meta.get("large") else None)
         return self._image
 
     @property

@@ -19,7 +19,7 @@ def index_for(g):
     return _ix[g.name]
 
 
-@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("case", golden_cases(large=True))
 @pytest.mark.parametrize("form", ["batched", "plain"])
 def test_gpu_matches_reference(golden, case, form):
     g = golden(case)
@@ -97,3 +97,25 @@ def test_logf_matches_host_libm_exhaustively(golden):
         host = O.logf_bits(a, n)
         mism = np.flatnonzero(dev.view(np.uint32) != host.view(np.uint32))
         assert len(mism) == 0, f"{len(mism)} mismatches from {a:#x}, first at {x[mism[0]]!r}"
+
+
+@pytest.mark.parametrize("case", ["uneven_small", "repeats_small", "long_small", "uneven_full"])
+def test_probe_layouts_agree(golden, case):
+    """The dual-strand tiers probe the hash-slot table (count, offset and first 7 postings per
+    hash) or the directory and postings arrays; both give the reference's results bit for bit,
+    on small indexes (slots forced on) and on the full-scale one (slots forced off)."""
+    g = golden(case)
+    ix = index_for(g)
+    was = bool(ix.info()["probe_slots"])
+    try:
+        out = {}
+        for on in (not was, was):
+            ix.set_probe_slots(on)
+            assert bool(ix.info()["probe_slots"]) == on
+            out[on] = ix.classify(g.reads.data, g.reads.offs)
+        assert np.array_equal(out[True].reads.view(np.uint8), out[False].reads.view(np.uint8))
+        assert np.array_equal(out[True].cands.view(np.uint8), out[False].cands.view(np.uint8))
+        d = diff(canon_from_gpu(out[True]), canon_from_dump(g.dump))
+        assert not d, "\n".join(d)
+    finally:
+        ix.set_probe_slots(was)

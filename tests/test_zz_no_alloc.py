@@ -36,8 +36,10 @@ def _inputs(g, strands):
             np.array(refs, np.uint32), np.array(r_off, np.uint64), np.array(runs, np.uint32).reshape(-1))
 
 
-def _noalloc(ix, q_off, bases, c_off, refs, r_off, runs):
-    """One call of the no-allocation entry point; device buffers are made here, by the caller."""
+def _noalloc(ix, q_off, bases, c_off, refs, r_off, runs, stream=None, free_delta=None):
+    """One call of the no-allocation entry point; device buffers are made here, by the caller.
+    stream: a torch.cuda.Stream to pass (None: the index's stream). free_delta: a list that
+    receives the change of the device's free memory across the call itself."""
     import torch
 
     dev = torch.device("cuda:0")
@@ -58,8 +60,12 @@ def _noalloc(ix, q_off, bases, c_off, refs, r_off, runs):
     fn = L.mg_score_candidates_noalloc
     fn.restype = C.c_int
     fn.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 11
+    free0 = torch.cuda.mem_get_info(dev)[0]
     rc = fn(ix.h, ns, *[t.data_ptr() for t in d], score.data_ptr(), pct.data_ptr(), rel.data_ptr(), hi.data_ptr(),
-            None)
+            stream.cuda_stream if stream is not None else None)
+    if free_delta is not None:
+        free_delta.append(torch.cuda.mem_get_info(dev)[0] - free0)
+    torch.cuda.synchronize()
     out = [t.cpu().numpy()[:n] for t, n in ((score, nc), (pct, nc), (rel, nc), (hi, ns))]
     return rc, out
 
@@ -82,6 +88,49 @@ def test_noalloc_matches_scoring_entry_point_twice(golden):
         assert int(args[2][-1]) > 100
         for w, o in zip(want, got):
             assert np.array_equal(_bits(w), _bits(o))
+
+
+def test_noalloc_allocates_nothing_and_takes_a_caller_stream(golden):
+    """After the first call on the device (which looks up the array's address), further calls
+    leave the device's free memory unchanged, on the index's stream and on a stream the caller
+    made, and give the same bits as the host-buffer entry point."""
+    import torch
+
+    g = golden("uneven_small")
+    ix = M.Index(g.image)
+    args = _inputs(g, g.dump.strands)
+    want = ix.score_candidates(*args)
+    rc, _ = _noalloc(ix, *args)  # set-up call
+    assert rc == 0, M.lib().mg_last_error()
+    side = torch.cuda.Stream()
+    for stream in (None, side, side):
+        delta = []
+        rc, got = _noalloc(ix, *args, stream=stream, free_delta=delta)
+        assert rc == 0, M.lib().mg_last_error()
+        assert delta == [0]
+        for w, o in zip(want, got):
+            assert np.array_equal(_bits(w), _bits(o))
+
+
+def test_both_scoring_entry_points_refuse_a_run_outside_its_query(golden):
+    """A run whose Last.Query lies beyond its query (or whose Start.Reference lies beyond its
+    reference) is refused with MG_ERR_INVAL by the host-buffer entry point before any copy and
+    by the no-allocation one on the device; neither writes outside its buffers."""
+    g = golden("uneven_small")
+    ix = M.Index(g.image)
+    s = next(x for x in g.dump.strands if x.cands and x.cands[0][4])
+    q_off, bases, c_off, refs, r_off, runs = _inputs(g, [s])
+    L = int(q_off[1])
+    for field, value in ((3, L + 40), (0, 0xFFFFFFF0)):
+        bad = runs.copy()
+        bad[field] = value
+        if field == 3:
+            bad[1] = min(int(bad[1]), L)  # keep Start.Query <= Last.Query: the run is walked
+        with pytest.raises(M.MirageError) as e:
+            ix.score_candidates(q_off, bases, c_off, refs, r_off, bad)
+        assert e.value.code == -8
+        rc, _ = _noalloc(ix, q_off, bases, c_off, refs, r_off, bad)
+        assert rc == -8, M.lib().mg_last_error()
 
 
 def test_noalloc_rejects_queries_beyond_its_limit(golden):
