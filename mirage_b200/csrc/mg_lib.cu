@@ -22,6 +22,7 @@
 #include "mg_kernels.cuh"
 #include "mg_lean.cuh"
 #include "mg_dual.cuh"
+#include "mg_long.cuh"
 #include "mhm.h"
 
 namespace mg {
@@ -387,6 +388,29 @@ __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp_list(DevIndex i
       }
     }
     __syncwarp();
+  }
+}
+
+// Long-read tier over the general warp tier's leftovers (reads beyond its limits), a block per
+// read with work stealing; its own leftovers go to the block tier.
+__global__ void __launch_bounds__(kLgThreads, 2) k_classify_long(DevIndex ix, BatchDev b, StageDev sd, const uint32_t* list,
+                                                              const unsigned* list_n, unsigned* cursor, uint32_t* next,
+                                                              unsigned* next_n) {
+  extern __shared__ __align__(16) uint8_t dsm[];
+  LongSmem& S = *reinterpret_cast<LongSmem*>(dsm);
+  __shared__ uint32_t s_item;
+  const uint32_t n = *list_n;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(cursor, 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    __syncthreads();
+    if (item >= n) break;
+    const uint32_t r = list[item];
+    if (!process_read_long(ix, b, r, S, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
+      if (threadIdx.x == 0) next[atomicAdd(next_n, 1u)] = r;
+    }
+    __syncthreads();
   }
 }
 
@@ -939,7 +963,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
   }
   if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
       w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
-      w.ovf.alloc(4 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+      w.ovf.alloc(5 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
@@ -947,7 +971,8 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 }
 
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
-// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovf0b | 60 work0b
+// 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovf0b | 60 work0b |
+// 64 n_ovf1b | 68 work of the long-read tier
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
                         bool plain, unsigned long long* chain, const ChainSync* cs) {
@@ -975,6 +1000,9 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   b.ovf0b = w.ovf.as<uint32_t>() + 3 * (n + 4);
   b.ovf1 = w.ovf.as<uint32_t>() + n + 4;
   b.ovf2 = w.ovf.as<uint32_t>() + 2 * (n + 4);
+  uint32_t* ovf1b = w.ovf.as<uint32_t>() + 4 * (n + 4);  // the long-read tier's leftovers
+  unsigned* n_ovf1b = (unsigned*)(ctr + 64);
+  unsigned* work_long = (unsigned*)(ctr + 68);
   StageDev sd;
   sd.stage = w.stage.as<mg_candidate>();
   sd.arena = w.arena.as<mg_candidate>();
@@ -988,6 +1016,7 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   static bool attr_set = false;
   if (!attr_set) {
     CU(cudaFuncSetAttribute(k_classify_block<kB2Threads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l2.total));
+    CU(cudaFuncSetAttribute(k_classify_long, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LongSmem)));
     attr_set = true;
   }
   const bool tm = ix->timing && ix->events_made;
@@ -1030,8 +1059,12 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
       k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, w.side>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[3], w.side));
+      int per_sm_long = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_long, k_classify_long, kLgThreads, sizeof(LongSmem));
+      k_classify_long<<<(unsigned)std::max(1, per_sm_long) * sms, kLgThreads, sizeof(LongSmem), w.side>>>(
+          ix->dix, b, sd, b.ovf1, b.n_ovf1, work_long, ovf1b, n_ovf1b);
       k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, w.side>>>(
-          ix->dix, b, sd, b.ovf1, b.n_ovf1, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
+          ix->dix, b, sd, ovf1b, n_ovf1b, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
       if (tm) CU(cudaEventRecord(ix->ev[4], w.side));
       global_tier(w.side);
       if (tm) CU(cudaEventRecord(ix->ev[5], w.side));

@@ -1,0 +1,349 @@
+// Long-read tier: reads longer than the warp tiers take (up to kLgQ bases), one block of
+// kLgThreads threads per read, both strands in turn, over reads taken from a list by work
+// stealing.
+//
+// The general path (process_strand, mg_kernels.cuh) sorts every posting of a strand twice:
+// by (refID, found index) for the occurrence filter and again, with the postings it dropped
+// padded in, by (refID, position, query position) for the diagonal runs. A 5 kb read has about
+// 750 postings per strand, a 20 kb read 3,000, while only the postings of the one or two
+// references with the longest occurrence runs survive the filter. Here the filter needs no sort:
+//   occurrence filter  every (refID, found index) pair of the strand goes into a hash set in
+//                      shared memory; a pair whose (refID, found index - 1) is absent starts an
+//                      occurrence run, whose length is the number of (refID, found index + t)
+//                      present after it; occMax of a reference is its longest run
+//                      (Analyser.cpp:2057-2115: consecutive found indices of one reference, a
+//                      reference counted once per found index), hs the longest of all
+//   keep rule          the references with a run of at least max(1, hs - 1) go to a small table
+//                      and only their postings are compacted (Analyser.cpp:2115-2196)
+//   sort               the kept postings only, by (refID, position, query position)
+// and the diagonal runs, the walks, the coverage and the scores follow as in process_strand
+// (Analyser.cpp:2337-2490, MatrixCPU.cpp:18-214), the coverage through a bitmap in shared memory.
+#pragma once
+#include "mg_kernels.cuh"
+
+namespace mg {
+
+constexpr int kLgThreads = 256;
+constexpr int kLgQ = 20480;     // longest read (the config's 20 kb reads)
+constexpr int kLgSeeds = 2047;  // seeds per strand (found index and seed index take 11 bits each)
+constexpr int kLgE = 4096;      // postings per strand
+constexpr int kLgK = 1024;      // kept postings per strand
+constexpr int kLgC = 64;        // scored candidates per strand
+constexpr int kLgRT = 128;      // table of kept references (at most half of it used)
+constexpr uint32_t kLgEmpty = 0xFFFFFFFFu;
+
+// Dynamic shared memory of one block. From the compaction on, the hash set holds the sort keys
+// (kA: kLgK uint64, kB: kLgK uint32), p_ref and p_pos the per-entry scratch X and Y, and p_fj
+// the coverage bitmap.
+struct alignas(16) LongSmem {
+  uint32_t hs[2 * kLgE];      // (refID << 11 | found index) set, open addressing
+  uint32_t p_ref[kLgE];       // the strand's postings in seed order
+  uint32_t p_pos[kLgE];
+  uint32_t p_fj[kLgE];        // found index | seed index << 11 | 1 << 31 for the pair's first posting
+  uint32_t rt[kLgRT];         // kept references
+  mg_candidate cb[2][kLgC];   // scored candidates of the two strands
+  RedTmp<kLgThreads> red;
+  uint32_t n_kept, n_rt;
+  uint8_t q[kLgQ];            // strand bases
+};
+static_assert(2 * sizeof(LongSmem) + 2048 <= 233472, "two blocks per SM");
+static_assert(kLgK * 12 <= 2 * kLgE * 4 && kLgQ / 32 + 1 <= kLgE, "aliased regions");
+
+__device__ __forceinline__ uint32_t lg_mix(uint32_t x) { return (x * 2654435761u) ^ (x >> 15); }
+
+__device__ __forceinline__ bool lg_contains(const uint32_t* set, uint32_t mask, uint32_t key) {
+  for (uint32_t s = lg_mix(key) & mask;; s = (s + 1) & mask) {
+    const uint32_t v = set[s];
+    if (v == key) return true;
+    if (v == kLgEmpty) return false;
+  }
+}
+
+// Inserts key; true when this call inserted it (false: it was there already).
+__device__ __forceinline__ bool lg_insert(uint32_t* set, uint32_t mask, uint32_t key) {
+  for (uint32_t s = lg_mix(key) & mask;; s = (s + 1) & mask) {
+    const uint32_t old = atomicCAS(&set[s], kLgEmpty, key);
+    if (old == kLgEmpty) return true;
+    if (old == key) return false;
+  }
+}
+
+// One strand of a read (raw bytes, L <= kLgQ) on the whole block. Same contract as
+// process_strand: kStrandOverflow hands the read to the block tier.
+__device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, int strand, LongSmem& S, int* err,
+                           uint32_t* n_out, float* highest) {
+  constexpr int G = kLgThreads;
+  const int tid = threadIdx.x;
+  const uint32_t k = (uint32_t)ix.k, step = (uint32_t)ix.step;
+  RedTmp<G>* red = &S.red;
+  *n_out = 0;
+  *highest = -1.0f;
+  // strand bases (A0)
+  uint32_t bad = 0;
+  for (uint32_t i = tid; i < L; i += G) {
+    uint8_t c;
+    if (strand == 0) {
+      c = upper_dev(raw[i]);
+    } else {
+      c = complement_dev(upper_dev(raw[L - 1 - i]));
+      if (!c) bad = 1;
+    }
+    S.q[i] = c;
+  }
+  if (grp_max_u64<G>(bad, red)) return kStrandBad;
+  if (L <= k) return kStrandOk;
+  const uint32_t ns = (L - k + step - 1) / step;
+  if (ns > (uint32_t)kLgSeeds) return kStrandOverflow;
+  // 1. seeds, probe, found indices, postings in seed order
+  uint32_t nf = 0, ne = 0;
+  for (uint32_t j0 = 0; j0 < ns; j0 += G) {
+    const uint32_t j = j0 + tid;
+    uint32_t found = 0, cnt = 0, o0 = 0;
+    uint4 v0 = make_uint4(0u, 0u, 0u, 0u), v1 = v0, v2 = v0, v3 = v0;
+    if (j < ns) {
+      const uint32_t h = hash28_dev(S.q + j * step, ix.hlen);
+      if (ix.slots) {
+        const uint4* sl = ix.slots + (size_t)h * kSlotVecs;
+        v0 = __ldg(sl);
+        v1 = __ldg(sl + 1);
+        cnt = v0.x;
+        o0 = v0.y;
+        if (cnt > 3) {
+          v2 = __ldg(sl + 2);
+          v3 = __ldg(sl + 3);
+        }
+      } else {
+        o0 = __ldg(ix.dir + h);
+        cnt = __ldg(ix.dir + h + 1) - o0;
+      }
+      found = (cnt > 0 || h == ix.empty_hash) ? 1u : 0u;
+    }
+    const uint32_t x = cnt > (uint32_t)kLgE ? (uint32_t)kLgE + 1 : cnt;
+    uint32_t fr, er;
+    const uint32_t fi = grp_excl_sum<G>(found, red, &fr);
+    const uint32_t ei = grp_excl_sum<G>(x, red, &er);
+    if (ne + er > (uint32_t)kLgE) return kStrandOverflow;  // group-uniform
+    const uint32_t e = ne + ei, fj = (nf + fi) | (j << 11);
+    uint32_t t0 = 0;
+    if (ix.slots) {
+      auto put = [&](uint32_t t, uint32_t ref, uint32_t pos) {
+        if (t < cnt) {
+          S.p_ref[e + t] = ref;
+          S.p_pos[e + t] = pos;
+          S.p_fj[e + t] = fj;
+        }
+      };
+      put(0, v0.z, v0.w);
+      put(1, v1.x, v1.y);
+      put(2, v1.z, v1.w);
+      put(3, v2.x, v2.y);
+      put(4, v2.z, v2.w);
+      put(5, v3.x, v3.y);
+      put(6, v3.z, v3.w);
+      t0 = kSlotPosts;
+    }
+    for (uint32_t t = t0; t < cnt; t++) {
+      const uint2 p = __ldg(ix.post + o0 + t);
+      S.p_ref[e + t] = p.x;
+      S.p_pos[e + t] = p.y;
+      S.p_fj[e + t] = fj;
+    }
+    nf += fr;
+    ne += er;
+  }
+  if (ne == 0) return kStrandOk;  // nothing found: the reference skips the strand
+  // 2. occurrence filter: the (refID, found index) set
+  uint32_t hsz = 64;
+  while (hsz < 2 * ne) hsz <<= 1;
+  const uint32_t mask = hsz - 1;
+  for (uint32_t i = tid; i < hsz; i += G) S.hs[i] = kLgEmpty;
+  for (uint32_t i = tid; i < (uint32_t)kLgRT; i += G) S.rt[i] = kLgEmpty;
+  if (tid == 0) {
+    S.n_kept = 0;
+    S.n_rt = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < ne; i += G)
+    if (lg_insert(S.hs, mask, (S.p_ref[i] << 11) | (S.p_fj[i] & 0x7FFu))) S.p_fj[i] |= 0x80000000u;
+  __syncthreads();
+  // occurrence runs from their first found index: the longest is hs
+  auto run_from = [&](uint32_t i) -> uint32_t {  // 0 unless posting i starts a run
+    const uint32_t fj = S.p_fj[i];
+    if (!(fj >> 31)) return 0;
+    const uint32_t key = (S.p_ref[i] << 11) | (fj & 0x7FFu);
+    if ((fj & 0x7FFu) && lg_contains(S.hs, mask, key - 1)) return 0;
+    uint32_t len = 1;
+    while ((fj & 0x7FFu) + len < nf && lg_contains(S.hs, mask, key + len)) len++;
+    return len;
+  };
+  uint32_t mx = 0;
+  for (uint32_t i = tid; i < ne; i += G) mx = max(mx, run_from(i));
+  const uint32_t hs = (uint32_t)grp_max_u64<G>(mx, red);
+  // hs only grows on a continued occurrence (Analyser.cpp:2087-2099): below 2 no reference can
+  // reach a diagonal run of 2 either, so the strand has no candidate
+  if (hs < 2) return kStrandOk;
+  const uint32_t keep_min = hs - 1;  // max(1, hs - 1), Analyser.cpp:2115
+  for (uint32_t i = tid; i < ne; i += G)
+    if (run_from(i) >= keep_min && lg_insert(S.rt, kLgRT - 1, S.p_ref[i])) atomicAdd(&S.n_rt, 1u);
+  __syncthreads();
+  if (S.n_rt > (uint32_t)kLgRT / 2) return kStrandOverflow;
+  // 3. the kept references' postings, as (refID << 32 | position, query position) sort keys
+  uint64_t* kA = reinterpret_cast<uint64_t*>(S.hs);
+  uint32_t* kB = S.hs + 2 * kLgK;
+  for (uint32_t i = tid; i < ne; i += G) {
+    const uint32_t ref = S.p_ref[i];
+    if (lg_contains(S.rt, kLgRT - 1, ref)) {
+      const uint32_t t = atomicAdd(&S.n_kept, 1u);
+      if (t < (uint32_t)kLgK) {
+        kA[t] = ((uint64_t)ref << 32) | S.p_pos[i];
+        kB[t] = ((S.p_fj[i] >> 11) & 0x7FFu) * step;
+      }
+    }
+  }
+  __syncthreads();
+  const int T2 = (int)S.n_kept;
+  if (T2 > kLgK) return kStrandOverflow;
+  const int N = next_pow2(T2);
+  for (int i = T2 + tid; i < N; i += G) {
+    kA[i] = ~0ull;
+    kB[i] = ~0u;
+  }
+  __syncthreads();
+  bitonic_sort<G>(kA, kB, N);
+  // 4. diagonal runs (Analyser.cpp:2337-2490): X = position within the run, Y = longest run of
+  //    the reference
+  uint32_t* X = S.p_ref;
+  uint32_t* Y = S.p_pos;
+  auto refA = [&](int i) { return (uint32_t)(kA[i] >> 32); };
+  auto rpos = [&](int i) { return (uint32_t)(kA[i] & 0xFFFFFFFFu); };
+  auto dbrk = [&](int i) {
+    return i == 0 || refA(i) != refA(i - 1) ||
+           !((uint64_t)rpos(i - 1) + step == rpos(i) && (uint64_t)kB[i - 1] + step == kB[i]);
+  };
+  auto rhead = [&](int i) { return i == 0 || refA(i) != refA(i - 1); };
+  auto rtail = [&](int i) { return i == T2 - 1 || refA(i) != refA(i + 1); };
+  arr_seg_scan<G, false>(X, T2, [&](int) -> uint32_t { return 1u; }, dbrk, OpAdd(), red);
+  arr_seg_scan<G, false>(Y, T2, [&](int i) -> uint32_t { return X[i]; }, rhead, OpMax(), red);
+  arr_seg_scan<G, true>(Y, T2, [&](int i) -> uint32_t { return Y[i]; }, rtail, OpMax(), red);
+  uint32_t mr = 0;
+  {
+    const int C = (T2 + G - 1) / G;
+    for (int i = tid * C; i < T2 && i < (tid + 1) * C; i++) mr = Y[i] > mr ? Y[i] : mr;
+  }
+  const uint32_t M = (uint32_t)grp_max_u64<G>(mr, red);
+  if (M < 2) return kStrandOk;  // Analyser.cpp:2402
+  // 5. head/tail walks of every run of a reference whose longest run is M: the run's covered
+  //    interval [Start.Q - head, Start.Q - head + T) and T go to X at the run's last entry
+  {
+    const int C = (T2 + G - 1) / G;
+    for (int i = tid * C; i < T2 && i < (tid + 1) * C; i++) {
+      uint32_t z = 0;
+      const bool rend = (i == T2 - 1) || dbrk(i + 1);
+      if (rend && Y[i] == M) {
+        const int s = i - (int)X[i] + 1;
+        const uint32_t ref = refA(i);
+        const uint32_t sr = rpos(s), sq = kB[s];
+        const uint32_t lr = rpos(i) + step, lq = kB[i] + step;
+        const uint8_t* rs = ix.bases + ix.ref_off[ref];
+        const uint32_t rlen = ix.ref_len[ref];
+        const uint32_t tail = tail_walk(S.q, rs, L, rlen, lq, lr, k);
+        const uint32_t head = head_walk(S.q, rs, sq, sr, k);
+        const uint32_t tot = tail + head + (lq - sq);
+        if (tot >= k) z = ((sq - head) << 16) | tot;
+      }
+      X[i] = z;
+    }
+  }
+  __syncthreads();
+  // 6. candidates in ascending refID: the heads of the reference segments whose longest run is M
+  uint32_t n_cand;
+  {
+    const int C = (T2 + G - 1) / G;
+    uint32_t local = 0;
+    for (int i = tid * C; i < T2 && i < (tid + 1) * C; i++) local += (rhead(i) && Y[i] == M);
+    uint32_t at = grp_excl_sum<G>(local, red, &n_cand);
+    __syncthreads();
+    for (int i = tid * C; i < T2 && i < (tid + 1) * C; i++)
+      if (rhead(i) && Y[i] == M) kB[at++] = (uint32_t)i;  // kB's query positions are walked by now
+  }
+  __syncthreads();
+  uint32_t* cov = S.p_fj;
+  const uint32_t nw = (L + 31) / 32;
+  uint32_t n_sc = 0;
+  float hi = -1.0f;
+  for (uint32_t c = 0; c < n_cand; c++) {
+    const int sa = (int)kB[c];
+    const uint32_t ref = refA(sa);
+    uint32_t first = (uint32_t)T2;
+    for (int i = sa + 1 + tid; i < T2; i += G)
+      if (refA(i) != ref) {
+        first = (uint32_t)i;
+        break;
+      }
+    const int sb = (int)(uint32_t)(~grp_max_u64<G>(~(uint64_t)first, red));  // group min
+    uint64_t sc = 0, sr = 0;
+    for (int i = sa + tid; i < sb; i += G) {
+      const uint32_t z = X[i];
+      if (z) {
+        const uint64_t t = z & 0xFFFFu;
+        sc += t;
+        sr += (t * (t + 1)) / 2;
+      }
+    }
+    for (uint32_t w = tid; w < nw; w += G) cov[w] = 0;
+    sc = grp_sum_u64<G>(sc, red);  // its barriers order the clear before the marks below
+    sr = grp_sum_u64<G>(sr, red);
+    if (sc == 0) continue;  // Score stays -2
+    for (int i = sa + tid; i < sb; i += G) {
+      const uint32_t z = X[i];
+      if (!z) continue;
+      const uint32_t a = z >> 16, bnd = a + (z & 0xFFFFu);
+      for (uint32_t wd = a >> 5; wd <= (bnd - 1) >> 5; wd++) {
+        const uint32_t w0 = wd * 32;
+        const uint32_t lo = a > w0 ? a : w0, up = bnd < w0 + 32 ? bnd : w0 + 32;
+        const uint32_t n = up - lo;
+        atomicOr(&cov[wd], (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0));
+      }
+    }
+    __syncthreads();
+    uint32_t hits = 0;
+    for (uint32_t w = tid; w < nw; w += G) hits += __popc(cov[w]);
+    hits = (uint32_t)grp_sum_u64<G>(hits, red);
+    float score, pct;
+    final_score(sr, sc, hits, L, &score, &pct);
+    const float rel = relative_score(ix, __uint2float_rn(L), __uint2float_rn(ix.ref_len[ref]), score, err);
+    if (n_sc >= (uint32_t)kLgC) return kStrandOverflow;
+    if (tid == 0) S.cb[strand][n_sc] = mg_candidate{ref, rel, score, pct};
+    n_sc++;
+    if (rel > hi) hi = rel;
+  }
+  __syncthreads();
+  *n_out = n_sc;
+  *highest = hi;
+  return kStrandOk;
+}
+
+// Both strands of read r, the strand merge and the staging write; false when the read must go
+// to the block tier.
+__device__ bool process_read_long(const DevIndex& ix, const BatchDev& b, uint32_t r, LongSmem& S, mg_candidate* stage,
+                                  mg_candidate* arena, uint64_t arena_cap, unsigned long long* arena_n, int* errw) {
+  const uint64_t o0 = b.offs[r];
+  const uint64_t Lr = b.offs[r + 1] - o0;
+  if (Lr > (uint64_t)kLgQ || ix.n_refs > (1u << 21)) return false;  // keys hold refID << 11
+  const uint32_t L = (uint32_t)Lr;
+  const uint8_t* raw = b.bases + o0;
+  int err = 0;
+  uint32_t n[2] = {0, 0};
+  float h[2] = {-1.0f, -1.0f};
+  int st = long_strand(ix, raw, L, 0, S, &err, &n[0], &h[0]);
+  if (st == kStrandOverflow) return false;
+  if (st != kStrandBad) st = long_strand(ix, raw, L, 1, S, &err, &n[1], &h[1]);
+  if (st == kStrandOverflow) return false;
+  if (threadIdx.x == 0)
+    write_read_result_s(b, r, st == kStrandBad, n[0], n[1], h[0], h[1], S.cb[0], S.cb[1], stage, arena, arena_cap,
+                        arena_n, errw, err);
+  __syncthreads();
+  return true;
+}
+
+}  // namespace mg

@@ -239,3 +239,34 @@ def test_chunked_batch_staging_overflow_runs_whole(tmp_path):
     a = gix.classify(data, roffs)
     assert (a.reads["n_fwd"] + a.reads["n_rc"]).sum() >= 24 * 270000
     _same(a, gix.classify(data, roffs, form="plain"))
+
+
+def test_long_read_tier_and_its_hand_offs(tmp_path):
+    """Reads of 400 bases to 20 kb on four identical references (every posting of a read's
+    true region kept four times) and one unrelated one: the long-read tier scores the reads
+    whose kept postings fit it (up to 1,024 per strand), hands longer ones to the block tier
+    (more kept postings) and to the global-memory tier (more than 4,096 postings per strand),
+    with errors and lowercase bases in some reads; every result equals the oracle's."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(43)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 40000)]
+    refs = [core] * 4 + [acgt[rng.integers(0, 4, 40000)]]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))])
+    path = tmp_path / "four.mhm"
+    image.tofile(path)
+    gix = M.Index(image)
+    oix = O.Index(str(path))
+    seqs = []
+    for n in (400, 1000, 2500, 3800, 4000, 6000, 12000, 20000):
+        s0 = int(rng.integers(0, 40000 - n))
+        r = core[s0:s0 + n].copy()
+        hit = rng.random(n) < 0.02  # substitutions: broken seeds, shorter occurrence runs
+        r[hit] = acgt[(np.searchsorted(acgt, r[hit]) + 1) % 4]
+        seqs.append(r.tobytes())
+        seqs.append(r.tobytes().lower())
+    seqs.append(refs[4][1000:9000].tobytes())
+    check_against_oracle(gix, oix, seqs)

@@ -29,7 +29,7 @@ def test_gpu_matches_reference(golden, case, form):
     assert not d, "\n".join(d)
 
 
-@pytest.mark.parametrize("case", ["plain", "uneven_small"])
+@pytest.mark.parametrize("case", ["plain", "uneven_small", "long_small"])
 def test_forms_agree_bitwise(golden, case):
     g = golden(case)
     ix = index_for(g)
