@@ -143,6 +143,27 @@ int mg_set_timing(mg_index* ix, int on);
  * indexes of at least 2^25 postings. Results are the same either way. Waits for the device to be
  * idle; MG_ERR_BUSY while a server (mg_server_create) is attached to the index. */
 int mg_set_probe_slots(mg_index* ix, int on);
+
+/* Launch shapes of the batched and served forms. They replace the reference's work balancing
+ * (Hardware::TryAutoIncreaseBlocksize and HardwareAutoConfigure, Hardware.cpp:138-228, which
+ * size its CPU and GPU batches at run time); results do not depend on them. A zero field keeps
+ * the library's default. mg_open sets them from the tuning file of the GPU model (written by
+ * python -m mirage_b200.tune) when one holds an entry for the index's density class
+ * (postings per 28-bit hash: sparse below 0.25, dense below 4, saturated from 4 on). */
+typedef struct {
+  uint32_t dual_blocks_per_sm;   /* resident 8-warp blocks per SM of the first dual-strand tier (1-5) */
+  uint32_t steal_chunk;          /* reads a warp of that tier takes per work-stealing step (1-64) */
+  uint32_t first_tier;           /* 1: the 64-posting dual-strand tier first (default); 2: reads start at
+                                  * the 128-posting tier (indexes whose strands mostly exceed 64 postings) */
+  uint32_t second_blocks_per_sm; /* 4-warp blocks per SM of the 128-posting tier (1-6) */
+  uint32_t finish_blocks_per_sm; /* 256-thread blocks per SM of the dual tiers' finishing pass (1-8) */
+  uint32_t long_blocks_per_sm;   /* blocks per SM of the long-read tier (1-2) */
+  uint32_t chunks;               /* pieces of a large host-buffer batch in mg_classify (1-8) */
+  uint32_t weighted_chunks;      /* 1: 8 chunks weighted 1-2-3-3-3-3-2-1; 2: equal chunks */
+} mg_tuning;
+int mg_set_tuning(mg_index* ix, const mg_tuning* t);
+/* The launch shapes in effect (defaults filled in) and the density class used to pick them. */
+int mg_get_tuning(const mg_index* ix, mg_tuning* t, char* density_class, uint64_t class_len);
 /* Diagnostic (no counterpart in the reference): the roofline of the lookup path. Times 2^26
  * gathers of whole 32-byte sectors (8 lanes per sector) at pseudo-random positions of a device
  * buffer of the largest power of two <= buffer_bytes (use several times the L2 size) on

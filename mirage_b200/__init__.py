@@ -24,7 +24,7 @@ ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LI
           -6: "MG_ERR_BADINPUT", -7: "MG_ERR_TIMEOUT", -8: "MG_ERR_INVAL", -9: "MG_ERR_BUSY"}
 
 EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
-           "mg_set_timing", "mg_set_probe_slots", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
+           "mg_set_timing", "mg_set_probe_slots", "mg_set_tuning", "mg_get_tuning", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
            "mg_build_image", "mg_build_image_device", "mg_parse_fasta_device", "mg_seqs_free", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_poll",
@@ -55,6 +55,14 @@ class _Info(C.Structure):
     _fields_ = [("n_hashes", C.c_uint64), ("n_postings", C.c_uint64), ("n_refs", C.c_uint64),
                 ("ref_bases", C.c_uint64), ("device_bytes", C.c_uint64), ("k", C.c_int32), ("word", C.c_int32),
                 ("load_seconds", C.c_double), ("upload_seconds", C.c_double), ("probe_slots", C.c_int32)]
+
+
+TUNING_FIELDS = ("dual_blocks_per_sm", "steal_chunk", "first_tier", "second_blocks_per_sm", "finish_blocks_per_sm",
+                 "long_blocks_per_sm", "chunks", "weighted_chunks")
+
+
+class _Tuning(C.Structure):
+    _fields_ = [(f, C.c_uint32) for f in TUNING_FIELDS]
 
 
 class _ServerConfig(C.Structure):
@@ -100,6 +108,8 @@ def lib() -> C.CDLL:
         L.mg_server_destroy.restype = None
         L.mg_set_timing.argtypes = [vp, i32]
         L.mg_set_probe_slots.argtypes = [vp, i32]
+        L.mg_set_tuning.argtypes = [vp, C.POINTER(_Tuning)]
+        L.mg_get_tuning.argtypes = [vp, C.POINTER(_Tuning), C.c_char_p, u64]
         L.mg_gather_bandwidth.argtypes = [i32, u64, C.POINTER(C.c_double)]
         L.mg_last_kernel_times.argtypes = [vp, vp]
         L.mg_bucket_sizes.argtypes = [vp, vp, vp, u64]
@@ -294,6 +304,18 @@ class Index:
     def set_probe_slots(self, on: bool = True) -> None:
         """Build (or drop) the hash-slot table the dual-strand tiers probe (mg_set_probe_slots)."""
         _check(lib().mg_set_probe_slots(self.h, 1 if on else 0), "mg_set_probe_slots")
+
+    def set_tuning(self, **fields) -> None:
+        """Launch shapes (mg_set_tuning); unnamed fields (and zeros) keep the defaults."""
+        t = _Tuning(*[int(fields.get(f, 0)) for f in TUNING_FIELDS])
+        _check(lib().mg_set_tuning(self.h, C.byref(t)), "mg_set_tuning")
+
+    def get_tuning(self) -> tuple[dict, str]:
+        """The launch shapes in effect and the index's density class (mg_get_tuning)."""
+        t = _Tuning()
+        cls = C.create_string_buffer(32)
+        _check(lib().mg_get_tuning(self.h, C.byref(t), cls, 32), "mg_get_tuning")
+        return {f: int(getattr(t, f)) for f in TUNING_FIELDS}, cls.value.decode()
 
     def set_timing(self, on: bool = True) -> None:
         _check(lib().mg_set_timing(self.h, 1 if on else 0), "mg_set_timing")

@@ -109,6 +109,7 @@ struct mg_index {
   bool chunk_made = false;
   std::mutex mu;
   std::atomic<int> n_servers{0};  // mg_server objects attached to this index
+  mg_tuning tune{};               // launch shapes (mg_set_tuning); zero fields: defaults
   mg_index_info info{};
   uint64_t device_bytes = 0;
   // optional per-kernel timing of the last pipeline (events on the launching stream)

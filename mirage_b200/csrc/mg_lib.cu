@@ -4,6 +4,8 @@
 
 #include <cub/device/device_scan.cuh>
 
+#include <dlfcn.h>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -50,7 +52,7 @@ int set_error(int code, const std::string& msg) {
 // the general warp tier takes its leftovers within the limits below.
 constexpr int kW1Warps = 8;
 constexpr int kW1Q = 320, kW1Seeds = 20, kW1E = 128, kW1C = 8;
-constexpr int kW1Chunk = 4;  // reads taken per work-stealing step
+constexpr int kW1Chunk = 4;  // reads taken per work-stealing step (default)
 
 struct WarpSmem {
   uint64_t kA[kW1E];
@@ -118,7 +120,7 @@ struct StageDev {
 
 // Dual-strand warp tier: every read of the batch, one warp per read (a half-warp per strand),
 // work stealing in chunks of kW1Chunk reads; reads that do not fit go to the general warp tier.
-__global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix, BatchDev b, StageDev sd) {
+__global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix, BatchDev b, StageDev sd, uint32_t chunk) {
   __shared__ DualSmem sm[kW1Warps];
   __shared__ uint8_t comp[256];
   for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
@@ -127,10 +129,10 @@ __global__ void __launch_bounds__(kW1Warps * 32, 5) k_classify_dual(DevIndex ix,
   DualSmem& S = sm[w];
   for (;;) {
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(b.work, (unsigned)kW1Chunk);
+    if (lane == 0) base = atomicAdd(b.work, chunk);
     base = __shfl_sync(0xffffffffu, base, 0);
     if ((uint64_t)base >= b.n) break;
-    const uint64_t end64 = (uint64_t)base + kW1Chunk;
+    const uint64_t end64 = (uint64_t)base + chunk;
     const uint32_t end = (uint32_t)(end64 < b.n ? end64 : b.n);
     for (uint32_t r = base; r < end; r++) {
       if (!process_read_dual(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
@@ -334,20 +336,22 @@ __global__ void __launch_bounds__(kFinThreads) k_finish_dual(DevIndex ix, BatchD
 // most 64 of them kept); the reads it takes leave run records for k_finish_dual like the first
 // tier's, its own leftovers go to the general warp tier. 4 warps per block (35 KB of shared memory).
 constexpr int kW2Warps = 4;
-__global__ void __launch_bounds__(kW2Warps * 32) k_classify_dual_list(DevIndex ix, BatchDev b, StageDev sd) {
+// With all_reads it takes every read of the batch (the first tier is not run).
+__global__ void __launch_bounds__(kW2Warps * 32) k_classify_dual_list(DevIndex ix, BatchDev b, StageDev sd,
+                                                                     int all_reads) {
   __shared__ DualSmemT<128> sm[kW2Warps];
   __shared__ uint8_t comp[256];
   for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   DualSmemT<128>& S = sm[w];
-  const uint32_t n = *b.n_ovf0;
+  const uint32_t n = all_reads ? (uint32_t)b.n : *b.n_ovf0;
   for (;;) {
     uint32_t item = 0;
     if (lane == 0) item = atomicAdd(b.work0b, 1u);
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= n) break;
-    const uint32_t r = b.ovf0[item];
+    const uint32_t r = all_reads ? item : b.ovf0[item];
     if (!process_read_dual(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
       if (lane == 0) {
         unsigned at = atomicAdd(b.n_ovf0b, 1u);
@@ -930,6 +934,8 @@ static int upload_index_image(mg_index* ix, const uint8_t* image, uint64_t L, co
   return build_log_table(ix);
 }
 
+static void load_tuning(mg_index* ix);
+
 static int open_image(mg_index* ix, const uint8_t* image, uint64_t L, int k, int device) {
   ix->device = device;
   CU(cudaSetDevice(device));
@@ -949,10 +955,110 @@ static int open_image(mg_index* ix, const uint8_t* image, uint64_t L, int k, int
   ix->info.n_refs = ix->host.n_refs;
   ix->info.ref_bases = meta.bases_len;
   ix->info.device_bytes = ix->device_bytes;
+  if (rc == MG_OK) load_tuning(ix);
   return rc;
 }
 
 // ---------------------------------------------------------------------- classification
+
+// ---------------------------------------------------------------------- launch shapes
+
+// The launch shapes in effect: mg_tuning's fields with the defaults filled in and clamped to what
+// the kernels can be launched with.
+struct Shapes {
+  unsigned dual_blocks_per_sm, steal_chunk, first_tier, second_blocks_per_sm, finish_blocks_per_sm,
+      long_blocks_per_sm, chunks, weighted_chunks;
+};
+
+static int occupancy(const void* fn, int threads, size_t smem) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem);
+  return std::max(1, n);
+}
+
+static Shapes shapes(const mg_index* ix) {
+  static int occ_dual = 0, occ_second = 0, occ_long = 0;
+  if (!occ_dual) {
+    cudaFuncSetAttribute(k_classify_long, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LongSmem));
+    occ_second = occupancy((const void*)k_classify_dual_list, kW2Warps * 32, 0);
+    occ_long = occupancy((const void*)k_classify_long, kLgThreads, sizeof(LongSmem));
+    occ_dual = occupancy((const void*)k_classify_dual, kW1Warps * 32, 0);
+  }
+  const mg_tuning& t = ix->tune;
+  auto pick = [](uint32_t v, unsigned def, unsigned lo, unsigned hi) {
+    return v ? std::min<unsigned>(hi, std::max<unsigned>(lo, v)) : def;
+  };
+  Shapes s;
+  s.first_tier = pick(t.first_tier, 1, 1, 2);
+  s.dual_blocks_per_sm = pick(t.dual_blocks_per_sm, (unsigned)occ_dual, 1, (unsigned)occ_dual);
+  s.steal_chunk = pick(t.steal_chunk, kW1Chunk, 1, 64);
+  // the 128-posting tier takes the first tier's few leftovers (one block per SM), or every read
+  s.second_blocks_per_sm = pick(t.second_blocks_per_sm, s.first_tier == 2 ? (unsigned)occ_second : 1u, 1,
+                                (unsigned)occ_second);
+  s.finish_blocks_per_sm = pick(t.finish_blocks_per_sm, 8, 1, 8);
+  s.long_blocks_per_sm = pick(t.long_blocks_per_sm, (unsigned)occ_long, 1, (unsigned)occ_long);
+  s.chunks = pick(t.chunks, mg_index::kMaxChunks, 1, mg_index::kMaxChunks);
+  s.weighted_chunks = pick(t.weighted_chunks, 1, 1, 2);
+  return s;
+}
+
+// Density class of an index (postings per 28-bit hash), the key of the tuning file's entries.
+static const char* density_class(uint64_t n_postings) {
+  const double d = (double)n_postings / (double)(1ull << 28);
+  return d < 0.25 ? "sparse" : d < 4.0 ? "dense" : "saturated";
+}
+
+// Launch shapes from the tuning file of this GPU model: MG_TUNING_FILE, else
+// tuning/<device name, spaces as '_'>.txt beside the library. A line "<class> key=value ..."
+// sets the fields it names for indexes of that density class; '#' starts a comment.
+static void load_tuning(mg_index* ix) {
+  std::string path;
+  if (const char* e = std::getenv("MG_TUNING_FILE")) {
+    path = e;
+  } else {
+    Dl_info info;
+    if (!dladdr((const void*)&load_tuning, &info) || !info.dli_fname) return;
+    std::string lib = info.dli_fname;
+    const size_t slash = lib.rfind('/');
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, ix->device) != cudaSuccess) return;
+    std::string name = p.name;
+    for (char& c : name)
+      if (c == ' ' || c == '/') c = '_';
+    path = (slash == std::string::npos ? std::string(".") : lib.substr(0, slash)) + "/tuning/" + name + ".txt";
+  }
+  std::ifstream f(path);
+  if (!f) return;
+  const std::string cls = density_class(ix->info.n_postings);
+  std::string line;
+  while (std::getline(f, line)) {
+    const size_t hash = line.find('#');
+    if (hash != std::string::npos) line.resize(hash);
+    size_t p = line.find_first_not_of(" \t");
+    if (p == std::string::npos) continue;
+    size_t q = line.find_first_of(" \t", p);
+    if (line.substr(p, q == std::string::npos ? std::string::npos : q - p) != cls) continue;
+    while (q != std::string::npos) {
+      p = line.find_first_not_of(" \t", q);
+      if (p == std::string::npos) break;
+      q = line.find_first_of(" \t", p);
+      const std::string kv = line.substr(p, q == std::string::npos ? std::string::npos : q - p);
+      const size_t eq = kv.find('=');
+      if (eq == std::string::npos) continue;
+      const std::string k = kv.substr(0, eq);
+      const uint32_t v = (uint32_t)std::strtoul(kv.c_str() + eq + 1, nullptr, 10);
+      mg_tuning& t = ix->tune;
+      if (k == "dual_blocks_per_sm") t.dual_blocks_per_sm = v;
+      else if (k == "steal_chunk") t.steal_chunk = v;
+      else if (k == "first_tier") t.first_tier = v;
+      else if (k == "second_blocks_per_sm") t.second_blocks_per_sm = v;
+      else if (k == "finish_blocks_per_sm") t.finish_blocks_per_sm = v;
+      else if (k == "long_blocks_per_sm") t.long_blocks_per_sm = v;
+      else if (k == "chunks") t.chunks = v;
+      else if (k == "weighted_chunks") t.weighted_chunks = v;
+    }
+  }
+}
 
 int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host_io) {
   uint64_t arena_cap = std::max<uint64_t>(1 << 16, n_reads * 2);
@@ -1046,10 +1152,11 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
         CU(cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&w.join, cudaEventDisableTiming));
       }
-      int per_sm1 = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_classify_dual, kW1Warps * 32, 0);
-      k_classify_dual<<<(unsigned)std::max(1, per_sm1) * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd);
-      k_classify_dual_list<<<(unsigned)sms, kW2Warps * 32, 0, st>>>(ix->dix, b, sd);
+      const Shapes sh = shapes(ix);
+      if (sh.first_tier == 1)
+        k_classify_dual<<<sh.dual_blocks_per_sm * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd, sh.steal_chunk);
+      k_classify_dual_list<<<sh.second_blocks_per_sm * sms, kW2Warps * 32, 0, st>>>(ix->dix, b, sd,
+                                                                                     sh.first_tier == 2);
       // the reads the dual tiers handed on go through the other tiers on the side stream, beside
       // the dual tier's finishing pass (different reads, disjoint slots; arena space by atomics)
       CU(cudaEventRecord(w.fork, st));
@@ -1059,9 +1166,7 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
       k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, w.side>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[3], w.side));
-      int per_sm_long = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_long, k_classify_long, kLgThreads, sizeof(LongSmem));
-      k_classify_long<<<(unsigned)std::max(1, per_sm_long) * sms, kLgThreads, sizeof(LongSmem), w.side>>>(
+      k_classify_long<<<sh.long_blocks_per_sm * sms, kLgThreads, sizeof(LongSmem), w.side>>>(
           ix->dix, b, sd, b.ovf1, b.n_ovf1, work_long, ovf1b, n_ovf1b);
       k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, w.side>>>(
           ix->dix, b, sd, ovf1b, n_ovf1b, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
@@ -1069,8 +1174,9 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       global_tier(w.side);
       if (tm) CU(cudaEventRecord(ix->ev[5], w.side));
       CU(cudaEventRecord(w.join, w.side));
-      k_finish_dual<<<(unsigned)std::min<uint64_t>((n + kFinThreads - 1) / kFinThreads, (uint64_t)sms * 8), kFinThreads, 0,
-                      st>>>(ix->dix, b, sd);
+      k_finish_dual<<<(unsigned)std::min<uint64_t>((n + kFinThreads - 1) / kFinThreads,
+                                                   (uint64_t)sms * sh.finish_blocks_per_sm),
+                      kFinThreads, 0, st>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[1], st));
       CU(cudaStreamWaitEvent(st, w.join, 0));
     }
@@ -1158,13 +1264,14 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
     ix->chunk_made = true;
   }
   if (w.chain.alloc(16)) return set_error(MG_ERR_OOM, "chunk counters");
-  const int nc = (int)std::min<uint64_t>(mg_index::kMaxChunks, n / kChunkReads);
+  const Shapes sh = shapes(ix);
+  const int nc = (int)std::min<uint64_t>(sh.chunks, n / kChunkReads);
   // chunk boundaries, weighted so that the first chunk (whose upload nothing hides) and the last
   // (whose classification and copy back nothing hides) are the smallest
   static const int kWeight[mg_index::kMaxChunks] = {1, 2, 3, 3, 3, 3, 2, 1};
   uint64_t bound[mg_index::kMaxChunks + 1];
   {
-    const bool weighted = nc == mg_index::kMaxChunks;
+    const bool weighted = nc == mg_index::kMaxChunks && sh.weighted_chunks == 1;
     uint64_t wsum = 0, acc = 0;
     for (int i = 0; i < nc; i++) wsum += weighted ? kWeight[i] : 1;
     bound[0] = 0;
@@ -1245,7 +1352,7 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   if (rc) return rc;
   if (w.cands.alloc(std::max<uint64_t>(out->cand_cap, 1) * sizeof(mg_candidate)))
     return set_error(MG_ERR_OOM, "candidate buffer");
-  if (!plain && n >= 2 * kChunkReads) {
+  if (!plain && n >= 2 * kChunkReads && shapes(ix).chunks > 1) {
     rc = classify_chunked(ix, w, batch, out);
     if (rc != kRunWhole) return rc;
   }
@@ -1417,6 +1524,23 @@ int mg_set_probe_slots(mg_index* ix, int on) {
   CU(cudaSetDevice(ix->device));
   CU(cudaDeviceSynchronize());  // no kernel of an earlier call still reads the table
   return set_probe_slots(ix, on != 0);
+}
+
+int mg_set_tuning(mg_index* ix, const mg_tuning* t) {
+  if (!ix || !t) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  ix->tune = *t;
+  return MG_OK;
+}
+
+int mg_get_tuning(const mg_index* ix, mg_tuning* t, char* cls, uint64_t cls_len) {
+  if (!ix || !t) return set_error(MG_ERR_INVAL, "null argument");
+  CU(cudaSetDevice(ix->device));
+  const Shapes s = shapes(ix);
+  *t = mg_tuning{s.dual_blocks_per_sm, s.steal_chunk, s.first_tier, s.second_blocks_per_sm,
+                 s.finish_blocks_per_sm, s.long_blocks_per_sm, s.chunks, s.weighted_chunks};
+  if (cls && cls_len) std::snprintf(cls, cls_len, "%s", density_class(ix->info.n_postings));
+  return MG_OK;
 }
 
 int mg_set_timing(mg_index* ix, int on) {
