@@ -256,18 +256,28 @@ int mg_score_candidates_noalloc(mg_index* ix, uint64_t n_strands, const uint64_t
                                 const uint32_t* d_runs, float* d_score, float* d_pct,
                                 float* d_rel, float* d_highest, void* stream);
 
-/* Served form: continuous batching against the HBM-resident index. Requests are admitted
- * into slots while device memory allows, coalesced into the running persistent kernel, and
- * completed independently. */
+/* Served form: continuous batching against the HBM-resident index (no counterpart in the
+ * reference). A request is admitted while it fits the pinned request ring, the tracked-request
+ * limit and the device-memory budget (its bases, offsets, read results and 8 candidates per read
+ * are booked until it completes; the budget follows the device's free memory as steps finish).
+ * Queued reads are coalesced into steps of the fused pipeline and requests complete
+ * independently. */
 typedef struct {
   uint32_t max_inflight_reads;  /* reads on the device at once (0: default) */
   uint32_t max_requests;        /* concurrently tracked requests (0: default) */
-  uint64_t device_budget;       /* bytes of device memory for request buffers (0: from free memory) */
+  uint64_t device_budget;       /* bytes of device memory for request buffers (0: a quarter of the free memory) */
 } mg_server_config;
 
 int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out);
 /* Copies the batch; returns MG_ERR_BUSY when it cannot be admitted now (retry later). */
 int mg_server_submit(mg_server* s, const mg_batch* batch, uint64_t* ticket);
+/* mg_server_submit with the caller's result buffers: the server writes the request's read
+ * results into out->reads (n_reads entries, cand_off counted from out->cands[0]) and its
+ * candidates into out->cands as its steps finish, so completion copies nothing; the buffers must
+ * stay valid until mg_server_poll / mg_server_wait has returned the request (out may be NULL
+ * there; out->n_cands of the submitted struct receives the count). When the candidates exceed
+ * out->cand_cap the request completes with MG_ERR_OOM and n_cands holds the number needed. */
+int mg_server_submit_into(mg_server* s, const mg_batch* batch, mg_result* out, uint64_t* ticket);
 /* Non-blocking: returns 1 and fills out when the request is complete, 0 when not yet. */
 int mg_server_poll(mg_server* s, uint64_t ticket, mg_result* out);
 /* Blocking variant of mg_server_poll with a timeout in milliseconds (MG_ERR_TIMEOUT). */

@@ -27,7 +27,7 @@ EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_insp
            "mg_set_timing", "mg_set_probe_slots", "mg_set_tuning", "mg_get_tuning", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
            "mg_build_image", "mg_build_image_device", "mg_parse_fasta_device", "mg_seqs_free", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
-           "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_poll",
+           "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_submit_into", "mg_server_poll",
            "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error", "mg_logs_open", "mg_logs_write",
            "mg_logs_close", "mg_make_results_dir", "mg_index_reference"]
 
@@ -102,6 +102,7 @@ def lib() -> C.CDLL:
         L.mg_score_candidates_noalloc.argtypes = [vp, u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.mg_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
         L.mg_server_submit.argtypes = [vp, C.POINTER(_Batch), C.POINTER(u64)]
+        L.mg_server_submit_into.argtypes = [vp, C.POINTER(_Batch), C.POINTER(_Result), C.POINTER(u64)]
         L.mg_server_poll.argtypes = [vp, u64, C.POINTER(_Result)]
         L.mg_server_wait.argtypes = [vp, u64, C.POINTER(_Result), C.c_uint32]
         L.mg_server_destroy.argtypes = [vp]
@@ -391,6 +392,7 @@ class Server:
         _check(lib().mg_server_create(index.h, C.byref(cfg), C.byref(h)), "mg_server_create")
         self.h = h
         self._pending: dict[int, int] = {}
+        self._into: dict[int, tuple] = {}  # ticket -> (reads, cands, result struct) of submit_into
 
     def submit(self, bases, offsets) -> int | None:
         """Submit a request; returns its ticket, or None when it cannot be admitted now."""
@@ -405,7 +407,34 @@ class Server:
         self._pending[t.value] = n
         return t.value
 
+    def submit_into(self, bases, offsets, cand_cap: int | None = None) -> int | None:
+        """Submit a request whose results the server writes straight into buffers made here
+        (mg_server_submit_into); returns its ticket, or None when it cannot be admitted now."""
+        bases, offsets = _u8(bases), _u64(offsets)
+        n = len(offsets) - 1
+        cap = cand_cap if cand_cap is not None else max(1024, 8 * n)
+        reads = np.empty(n, dtype=READ_DTYPE)
+        cands = np.empty(cap, dtype=CAND_DTYPE)
+        res = _Result(reads.ctypes.data, cands.ctypes.data, cap, 0)
+        b = _Batch(n, offsets.ctypes.data, bases.ctypes.data)
+        t = C.c_uint64()
+        rc = lib().mg_server_submit_into(self.h, C.byref(b), C.byref(res), C.byref(t))
+        if rc == -9:
+            return None
+        _check(rc, "mg_server_submit_into")
+        self._into[t.value] = (reads, cands, res)
+        return t.value
+
     def _result(self, ticket: int, fn, *extra):
+        if ticket in self._into:
+            reads, cands, res = self._into[ticket]
+            rc = fn(self.h, ticket, None, *extra)
+            if rc != 0:
+                self._into.pop(ticket, None)
+            _check(rc, "mg_server_poll")
+            if rc == 0:
+                return None
+            return Results(reads, cands[: res.n_cands].copy())
         n = self._pending.get(ticket, 0)
         cap = max(1024, 8 * n)
         while True:

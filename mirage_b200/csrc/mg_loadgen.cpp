@@ -1,8 +1,9 @@
 // Load generator for the served form: client threads that drive an mg_server through the public
-// C ABI (mg_server_submit / mg_server_wait) the way a C++ caller would, for throughput and
+// C ABI (mg_server_submit_into / mg_server_wait) the way a C++ caller would, for throughput and
 // latency measurement. Requests are contiguous slices of a pool of reads, with log-uniform sizes
-// in [1, max_req] reads; each client rebases its slice's offsets into its own buffer, submits it
-// (which copies it) and collects the results into its own buffers.
+// in [1, max_req] reads; each client rebases its slice's offsets into its own buffer and submits
+// it (which copies it) with result buffers from its own pool, into which the server writes the
+// results; a request whose candidates overflow its buffer is submitted again with a larger one.
 //
 //   rate_reads_s == 0: closed loop, each client keeps `depth` requests outstanding
 //   rate_reads_s  > 0: open loop, Poisson arrivals split evenly over the clients; latency is
@@ -15,6 +16,7 @@
 #include <cstdint>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <random>
 #include <thread>
@@ -42,16 +44,24 @@ struct Pool {
   uint32_t max_req;
 };
 
+// Result buffers of one request, reused across requests (allocated and touched by the client,
+// so the server's delivery threads write into resident pages).
+struct Buf {
+  std::vector<mg_read_result> reads;
+  std::vector<mg_candidate> cands;
+  mg_result res{};
+  mg_batch batch{};
+};
+
 struct Client {
   std::mt19937_64 rng;
   std::vector<uint64_t> o;
-  std::vector<mg_read_result> reads;
-  std::vector<mg_candidate> cands;
   std::vector<double> lat_ms;
+  std::mutex pool_mu;
+  std::vector<std::unique_ptr<Buf>> pool;
   uint64_t reads_done = 0, requests = 0;
   int error = 0;
-  explicit Client(uint64_t seed, uint32_t max_req)
-      : rng(seed), o(max_req + 1), reads(max_req), cands((size_t)64 * max_req) {}
+  explicit Client(uint64_t seed, uint32_t max_req) : rng(seed), o(max_req + 1) {}
 
   // a request: (first read, size); its offsets rebased into o
   mg_batch draw(const Pool& p, uint32_t* size_out) {
@@ -65,48 +75,89 @@ struct Client {
     *size_out = (uint32_t)size;
     return mg_batch{size, o.data(), p.bases + b0};
   }
-  int submit(mg_server* sv, const mg_batch& b, uint64_t* t) {
+  Buf* acquire(uint64_t n, uint64_t n_cands) {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    for (size_t i = 0; i < pool.size(); i++)
+      if (pool[i]->reads.size() >= n && pool[i]->cands.size() >= n_cands) {
+        Buf* b = pool[i].release();
+        pool.erase(pool.begin() + (long)i);
+        return b;
+      }
+    Buf* b = new Buf();
+    uint64_t cap = 1;
+    while (cap < n) cap <<= 1;  // powers of two, so buffers are reused across sizes
+    b->reads.assign(cap, mg_read_result{});
+    b->cands.assign(std::max<uint64_t>(16 * cap + 64, n_cands), mg_candidate{});
+    return b;
+  }
+  void release(Buf* b) {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    pool.emplace_back(b);
+  }
+  int submit(mg_server* sv, const mg_batch& bt, Buf* b, uint64_t* t) {
+    b->batch = bt;
+    b->res = mg_result{b->reads.data(), b->cands.data(), b->cands.size(), 0};
     for (;;) {
-      const int rc = mg_server_submit(sv, &b, t);
+      const int rc = mg_server_submit_into(sv, &bt, &b->res, t);
       if (rc != MG_ERR_BUSY) return rc;
       std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
   }
-  int wait(mg_server* sv, uint64_t t) {
-    mg_result r{reads.data(), cands.data(), cands.size(), 0};
-    const int rc = mg_server_wait(sv, t, &r, 600000);
-    return rc == 1 ? MG_OK : (rc ? rc : MG_ERR_TIMEOUT);
+  // waits for the request; one whose candidates did not fit goes again with a larger buffer (its
+  // batch still points at the pool's reads; the rebased offsets are copied first)
+  int wait(mg_server* sv, uint64_t t, Buf*& b) {
+    for (;;) {
+      const int rc = mg_server_wait(sv, t, nullptr, 600000);
+      if (rc == 1) return MG_OK;
+      if (rc != MG_ERR_OOM || b->res.n_cands <= b->cands.size()) return rc ? rc : MG_ERR_TIMEOUT;
+      b->cands.assign(b->res.n_cands + 1024, mg_candidate{});
+      std::vector<uint64_t> offs(b->batch.offsets, b->batch.offsets + b->batch.n_reads + 1);
+      const mg_batch bt{b->batch.n_reads, offs.data(), b->batch.bases};
+      if (int s = submit(sv, bt, b, &t)) return s;
+    }
   }
 };
 
+// an outstanding request: ticket, (scheduled) submission time, reads, result buffers
+struct Out {
+  uint64_t ticket;
+  Clock::time_point t0;
+  uint32_t size;
+  Buf* buf;
+};
+
 void closed_loop(mg_server* sv, const Pool& p, Client& c, Clock::time_point end, int depth) {
-  std::deque<std::pair<uint64_t, std::pair<Clock::time_point, uint32_t>>> q;
+  std::deque<Out> q;
   while (Clock::now() < end && !c.error) {
     uint32_t size;
     const mg_batch b = c.draw(p, &size);
     uint64_t t;
+    Buf* buf = c.acquire(size, 16ull * size + 64);
     const auto t0 = Clock::now();
-    if (int rc = c.submit(sv, b, &t)) {
+    if (int rc = c.submit(sv, b, buf, &t)) {
+      c.release(buf);
       c.error = rc;
       break;
     }
-    q.push_back({t, {t0, size}});
+    q.push_back(Out{t, t0, size, buf});
     if ((int)q.size() >= depth) {
-      auto f = q.front();
+      Out f = q.front();
       q.pop_front();
-      if (int rc = c.wait(sv, f.first)) c.error = rc;
-      c.lat_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - f.second.first).count());
-      c.reads_done += f.second.second;
+      if (int rc = c.wait(sv, f.ticket, f.buf)) c.error = rc;
+      c.lat_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - f.t0).count());
+      c.reads_done += f.size;
       c.requests++;
+      c.release(f.buf);
     }
   }
   while (!q.empty()) {
-    auto f = q.front();
+    Out f = q.front();
     q.pop_front();
-    if (int rc = c.wait(sv, f.first)) c.error = c.error ? c.error : rc;
-    c.lat_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - f.second.first).count());
-    c.reads_done += f.second.second;
+    if (int rc = c.wait(sv, f.ticket, f.buf)) c.error = c.error ? c.error : rc;
+    c.lat_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - f.t0).count());
+    c.reads_done += f.size;
     c.requests++;
+    c.release(f.buf);
   }
 }
 
@@ -114,11 +165,11 @@ void open_loop(mg_server* sv, const Pool& p, Client& c, Clock::time_point start,
                double req_per_s) {
   std::mutex mu;
   std::condition_variable cv;
-  std::deque<std::pair<uint64_t, std::pair<Clock::time_point, uint32_t>>> q;
+  std::deque<Out> q;
   bool fin = false;
   std::thread waiter([&] {
     for (;;) {
-      std::pair<uint64_t, std::pair<Clock::time_point, uint32_t>> f;
+      Out f;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv.wait(lk, [&] { return fin || !q.empty(); });
@@ -126,10 +177,11 @@ void open_loop(mg_server* sv, const Pool& p, Client& c, Clock::time_point start,
         f = q.front();
         q.pop_front();
       }
-      if (int rc = c.wait(sv, f.first)) c.error = c.error ? c.error : rc;
-      c.lat_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - f.second.first).count());
-      c.reads_done += f.second.second;
+      if (int rc = c.wait(sv, f.ticket, f.buf)) c.error = c.error ? c.error : rc;
+      c.lat_ms.push_back(std::chrono::duration<double, std::milli>(Clock::now() - f.t0).count());
+      c.reads_done += f.size;
       c.requests++;
+      c.release(f.buf);
     }
   });
   std::exponential_distribution<double> gap(req_per_s);
@@ -142,13 +194,15 @@ void open_loop(mg_server* sv, const Pool& p, Client& c, Clock::time_point start,
     uint32_t size;
     const mg_batch b = c.draw(p, &size);
     uint64_t t;
-    if (int rc = c.submit(sv, b, &t)) {
+    Buf* buf = c.acquire(size, 16ull * size + 64);
+    if (int rc = c.submit(sv, b, buf, &t)) {
+      c.release(buf);
       c.error = rc;
       break;
     }
     {
       std::lock_guard<std::mutex> lk(mu);
-      q.push_back({t, {arrive, size}});
+      q.push_back(Out{t, arrive, size, buf});
     }
     cv.notify_one();
   }
@@ -168,25 +222,25 @@ extern "C" int mg_loadgen_run(mg_server* sv, const uint64_t* offs, const uint8_t
   if (!sv || !offs || !bases || !out || n_reads == 0 || clients < 1 || max_req < 1 || seconds <= 0)
     return MG_ERR_INVAL;
   Pool p{offs, bases, n_reads, (uint32_t)std::min<uint64_t>(max_req, n_reads)};
-  std::vector<Client> cl;
-  cl.reserve(clients);
-  for (int i = 0; i < clients; i++) cl.emplace_back(seed + 7919ull * (uint64_t)i, p.max_req);
+  std::vector<std::unique_ptr<Client>> cl;
+  for (int i = 0; i < clients; i++) cl.emplace_back(new Client(seed + 7919ull * (uint64_t)i, p.max_req));
   const double mean_size = p.max_req > 1 ? (double)(p.max_req - 1) / std::log((double)p.max_req) : 1.0;
   const auto t0 = Clock::now();
   std::vector<std::thread> th;
   for (int i = 0; i < clients; i++)
     th.emplace_back([&, i] {
       if (rate_reads_s > 0)
-        open_loop(sv, p, cl[i], t0, seconds, rate_reads_s / mean_size / clients);
+        open_loop(sv, p, *cl[i], t0, seconds, rate_reads_s / mean_size / clients);
       else
-        closed_loop(sv, p, cl[i], t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(seconds)),
+        closed_loop(sv, p, *cl[i], t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(seconds)),
                     std::max(1, depth));
     });
   for (auto& t : th) t.join();
   const double wall = std::chrono::duration<double>(Clock::now() - t0).count();
   std::vector<double> lat;
   std::memset(out, 0, sizeof(*out));
-  for (auto& c : cl) {
+  for (auto& cp : cl) {
+    const Client& c = *cp;
     lat.insert(lat.end(), c.lat_ms.begin(), c.lat_ms.end());
     out->reads += c.reads_done;
     out->requests += c.requests;

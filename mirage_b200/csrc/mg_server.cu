@@ -9,6 +9,12 @@
 // copies and kernels run while the previous step's results are drained. A request arriving
 // while steps are on the device joins the next step formed. Each read is classified on its
 // own, so a request's results are the same alone and in any mix.
+//
+// Admission also holds device memory: each admitted request books the device bytes its reads
+// take in a step (bases, offsets, results and a candidate allowance) against a budget, which
+// follows the device's free memory as steps complete (another user's allocations shrink it).
+// A request submitted with caller buffers (mg_server_submit_into) has its results written into
+// them by the server's delivery threads, with no copy at completion.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -38,6 +44,9 @@ struct Request {
   uint64_t done = 0;  // reads with results
   std::vector<mg_read_result> reads;
   std::vector<mg_candidate> cands;
+  mg_result* dst = nullptr;   // caller buffers (mg_server_submit_into), written as segments finish
+  uint64_t n_cands = 0;       // candidates delivered (or needed, when dst's capacity ran out)
+  uint64_t dev_bytes = 0;     // device bytes booked at admission
   int error = 0;
   bool complete = false;
   bool released = false;  // ring space returned
@@ -66,6 +75,9 @@ struct Slot {
 struct mg_server {
   mg_index* ix = nullptr;
   uint64_t step_reads = 0, step_bases = 0;
+  uint64_t dev_budget = 0, dev_booked = 0;  // admission: device bytes of the admitted requests
+  uint64_t dev_cap = 0;                     // the budget set at creation (the budget's ceiling)
+  uint64_t dev_reserve = 0;                 // free device memory kept for the step buffers' growth
   uint32_t max_requests = 0;
   mg::Ring ring;
   uint64_t next_ticket = 1;
@@ -225,18 +237,28 @@ static void drain_step(mg_server* sv, Slot& s) {
       return;
     }
     if (r->error) return;
-    // the segment's candidates are contiguous in the step's output (read order): one copy
+    // the segment's candidates are contiguous in the step's output (read order): one copy, into
+    // the caller's buffer when the request has one
     const mg_read_result* src = s.h_reads + at;
     const mg_read_result& last = src[p.count - 1];
     const uint64_t c0 = src[0].cand_off, c1 = (uint64_t)last.cand_off + last.n_fwd + last.n_rc;
-    const uint64_t base = r->cands.size();
-    try {
-      r->cands.insert(r->cands.end(), s.h_cands + c0, s.h_cands + c1);
-    } catch (...) {
-      r->error = MG_ERR_OOM;
-      return;
+    const uint64_t base = r->n_cands;
+    r->n_cands += c1 - c0;
+    if (r->dst) {
+      if (r->n_cands > r->dst->cand_cap) {
+        r->error = MG_ERR_OOM;  // n_cands keeps counting what the request needs
+        return;
+      }
+      if (c1 > c0) std::memcpy(r->dst->cands + base, s.h_cands + c0, (c1 - c0) * sizeof(mg_candidate));
+    } else {
+      try {
+        r->cands.insert(r->cands.end(), s.h_cands + c0, s.h_cands + c1);
+      } catch (...) {
+        r->error = MG_ERR_OOM;
+        return;
+      }
     }
-    mg_read_result* dst = r->reads.data() + p.first;
+    mg_read_result* dst = (r->dst ? r->dst->reads : r->reads.data()) + p.first;
     for (uint64_t i = 0; i < p.count; i++) {
       mg_read_result rr = src[i];
       if (rr.strand == MG_READ_BAD_BYTE || rr.strand == MG_READ_TOO_LARGE) {
@@ -247,11 +269,21 @@ static void drain_step(mg_server* sv, Slot& s) {
       dst[i] = rr;
     }
   };
+  // a request whose error came from an earlier segment still counts the candidates it needs
+  auto count_only = [&](const Part& p, uint64_t at) {
+    Request* r = p.req;
+    if (rc != MG_OK || !r->dst || r->error != MG_ERR_OOM) return false;
+    const mg_read_result* src = s.h_reads + at;
+    const mg_read_result& last = src[p.count - 1];
+    r->n_cands += (uint64_t)last.cand_off + last.n_fwd + last.n_rc - src[0].cand_off;
+    return true;
+  };
   const size_t np = s.parts.size();
   std::vector<uint64_t> start(np + 1, 0);
   for (size_t i = 0; i < np; i++) start[i + 1] = start[i] + s.parts[i].count;
   auto deliver_range = [&](size_t a, size_t b) {
-    for (size_t i = a; i < b; i++) deliver(s.parts[i], start[i]);
+    for (size_t i = a; i < b; i++)
+      if (!count_only(s.parts[i], start[i])) deliver(s.parts[i], start[i]);
   };
   // large steps: up to kDeliverThreads contiguous ranges of segments with about equal reads
   constexpr int kDeliverThreads = 4;
@@ -278,7 +310,14 @@ static void drain_step(mg_server* sv, Slot& s) {
     deliver_range(cut[0], cut[1]);
     for (std::thread& h : helpers) h.join();
   }
+  // the device budget follows the device's free memory (read outside the lock)
+  size_t free_b = 0, total_b = 0;
+  const bool have_free = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
   std::lock_guard<std::mutex> lk(sv->mu);
+  if (have_free) {
+    const uint64_t room = free_b > sv->dev_reserve ? free_b - sv->dev_reserve : 0;
+    sv->dev_budget = std::min(sv->dev_cap, room + sv->dev_booked);
+  }
   for (const Part& p : s.parts) {
     Request* r = p.req;
     r->done += p.count;
@@ -288,6 +327,8 @@ static void drain_step(mg_server* sv, Slot& s) {
         sv->ring.release(r->ring_at);
         r->released = true;
       }
+      sv->dev_booked -= r->dev_bytes;
+      r->dev_bytes = 0;
     }
   }
   s.parts.clear();
@@ -347,6 +388,8 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
   const uint64_t dev_budget = c.device_budget ? c.device_budget : (uint64_t)(free_b / 4);
   uint64_t reads = c.max_inflight_reads ? c.max_inflight_reads : 262144;
   reads = std::max<uint64_t>(1024, std::min<uint64_t>(reads, dev_budget / 2 / per_read));
+  sv->dev_cap = sv->dev_budget = dev_budget;
+  sv->dev_reserve = (uint64_t)(free_b / 8);  // kept free beyond the budget
   sv->step_reads = reads;
   sv->step_bases = reads * 320;
   sv->max_requests = c.max_requests ? c.max_requests : 4096;
@@ -371,8 +414,16 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
   return MG_OK;
 }
 
-int mg_server_submit(mg_server* sv, const mg_batch* b, uint64_t* ticket) {
+// Device bytes a request books: its bases and offsets on the device, its read results and an
+// allowance of 8 candidates per read (the step buffers grow beyond it when needed).
+static uint64_t request_device_bytes(uint64_t n, uint64_t nb) {
+  return nb + (n + 1) * 8 + n * (sizeof(mg_read_result) + 8 * sizeof(mg_candidate));
+}
+
+static int submit(mg_server* sv, const mg_batch* b, mg_result* dst, uint64_t* ticket) {
   if (!sv || !b || !ticket || (b->n_reads && (!b->offsets || !b->bases))) return set_error(MG_ERR_INVAL, "null argument");
+  if (dst && b->n_reads && (!dst->reads || (dst->cand_cap && !dst->cands)))
+    return set_error(MG_ERR_INVAL, "null output buffer");
   const uint64_t n = b->n_reads;
   const uint64_t nb = n ? b->offsets[n] : 0;
   if (n && b->offsets[0] != 0) return set_error(MG_ERR_INVAL, "offsets[0] must be 0");
@@ -382,22 +433,31 @@ int mg_server_submit(mg_server* sv, const mg_batch* b, uint64_t* ticket) {
   const uint64_t len = nb + (n + 1) * 8 + 16;
   std::unique_ptr<Request> r(new Request());
   r->n = n;
+  r->dst = dst;
+  const uint64_t dev = request_device_bytes(n, nb);
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     if (len > sv->ring.cap) return set_error(MG_ERR_LIMIT, "request larger than the server's request memory");
+    if (dev > sv->dev_cap) return set_error(MG_ERR_LIMIT, "request larger than the server's device budget");
+    if (sv->dev_booked + dev > sv->dev_budget) return set_error(MG_ERR_BUSY, "not enough free device memory now");
     if (sv->live.size() >= sv->max_requests || !sv->ring.alloc(len, &r->ring_at))
       return set_error(MG_ERR_BUSY, "server at capacity");
+    sv->dev_booked += dev;
+    r->dev_bytes = dev;
     r->offs = (uint64_t*)(sv->ring.base + r->ring_at);
     r->bases = sv->ring.base + r->ring_at + (n + 1) * 8;
   }
   std::memcpy(r->offs, b->offsets, (n + 1) * 8);
   std::memcpy(r->bases, b->bases, nb);
-  try {
-    r->reads.resize(n);
-  } catch (...) {
-    std::lock_guard<std::mutex> lk(sv->mu);
-    sv->ring.release(r->ring_at);
-    return set_error(MG_ERR_OOM, "host memory for the results");
+  if (!dst) {
+    try {
+      r->reads.resize(n);
+    } catch (...) {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->ring.release(r->ring_at);
+      sv->dev_booked -= dev;
+      return set_error(MG_ERR_OOM, "host memory for the results");
+    }
   }
   std::lock_guard<std::mutex> lk(sv->mu);
   r->ticket = sv->next_ticket++;
@@ -406,6 +466,8 @@ int mg_server_submit(mg_server* sv, const mg_batch* b, uint64_t* ticket) {
     r->complete = true;
     r->released = true;
     sv->ring.release(r->ring_at);
+    sv->dev_booked -= r->dev_bytes;
+    r->dev_bytes = 0;
   } else {
     sv->queue.push_back(r.get());
   }
@@ -414,11 +476,29 @@ int mg_server_submit(mg_server* sv, const mg_batch* b, uint64_t* ticket) {
   return MG_OK;
 }
 
+int mg_server_submit(mg_server* sv, const mg_batch* b, uint64_t* ticket) { return submit(sv, b, nullptr, ticket); }
+
+int mg_server_submit_into(mg_server* sv, const mg_batch* b, mg_result* out, uint64_t* ticket) {
+  if (!out) return set_error(MG_ERR_INVAL, "null output");
+  return submit(sv, b, out, ticket);
+}
+
 // Hand a completed request to its caller: detached from the server under the lock, copied out and
 // freed after the lock is released. A request whose candidates do not fit stays for a retry.
 static int take_result(mg_server* sv, std::map<uint64_t, std::unique_ptr<Request>>::iterator it, mg_result* out,
                        std::unique_lock<std::mutex>& lk) {
   Request* r0 = it->second.get();
+  if (r0->dst) {  // results are in the caller's buffers already
+    std::unique_ptr<Request> r = std::move(it->second);
+    sv->live.erase(it);
+    lk.unlock();
+    r->dst->n_cands = r->n_cands;
+    if (out) out->n_cands = r->n_cands;
+    if (r->error == MG_ERR_OOM) return set_error(MG_ERR_OOM, "candidate output buffer too small");
+    if (r->error) return set_error(r->error, mg_strerror(r->error));
+    return 1;
+  }
+  if (!out) return set_error(MG_ERR_INVAL, "null output");
   if (!r0->error && r0->cands.size() > out->cand_cap) {
     out->n_cands = r0->cands.size();
     return set_error(MG_ERR_OOM, "candidate output buffer too small");
@@ -434,7 +514,7 @@ static int take_result(mg_server* sv, std::map<uint64_t, std::unique_ptr<Request
 }
 
 int mg_server_poll(mg_server* sv, uint64_t ticket, mg_result* out) {
-  if (!sv || !out) return set_error(MG_ERR_INVAL, "null argument");
+  if (!sv) return set_error(MG_ERR_INVAL, "null argument");
   std::unique_lock<std::mutex> lk(sv->mu);
   auto it = sv->live.find(ticket);
   if (it == sv->live.end()) return set_error(MG_ERR_INVAL, "unknown ticket");
@@ -443,7 +523,7 @@ int mg_server_poll(mg_server* sv, uint64_t ticket, mg_result* out) {
 }
 
 int mg_server_wait(mg_server* sv, uint64_t ticket, mg_result* out, uint32_t timeout_ms) {
-  if (!sv || !out) return set_error(MG_ERR_INVAL, "null argument");
+  if (!sv) return set_error(MG_ERR_INVAL, "null argument");
   std::unique_lock<std::mutex> lk(sv->mu);
   auto it = sv->live.find(ticket);
   if (it == sv->live.end()) return set_error(MG_ERR_INVAL, "unknown ticket");

@@ -112,3 +112,57 @@ def test_admission_and_errors(golden):
     r = sv.wait(t)
     assert len(r.reads) == 0
     sv.close()
+
+
+def test_results_into_caller_buffers(golden):
+    """mg_server_submit_into: the server writes each request's results straight into the
+    caller's buffers; they equal the copying form's, alone and mixed with copied requests; a
+    candidate buffer too small completes its request with MG_ERR_OOM and the count it needs."""
+    g = golden("uneven_small")
+    ix = M.Index(g.image)
+    rng = np.random.default_rng(9)
+    cuts = np.unique(np.concatenate([[0, len(g.reads)], rng.integers(1, len(g.reads), size=30)]))
+    parts = split(g.reads, cuts)
+    alone = [ix.classify(d, o) for d, o in parts]
+    sv = M.Server(ix, max_inflight_reads=1024)
+    tickets = [sv.submit_into(d, o) if i % 2 == 0 else sv.submit(d, o) for i, (d, o) in enumerate(parts)]
+    assert all(t is not None for t in tickets)
+    for a, t in zip(alone, tickets):
+        same(a, sv.wait(t))
+    big = max(range(len(parts)), key=lambda i: len(alone[i].cands))
+    need = len(alone[big].cands)
+    assert need > 4
+    t = sv.submit_into(*parts[big], cand_cap=need // 2)
+    with pytest.raises(M.MirageError) as e:
+        sv.wait(t)
+    assert e.value.code == -3
+    t = sv.submit_into(*parts[big], cand_cap=need)
+    same(alone[big], sv.wait(t))
+    sv.close()
+
+
+def test_admission_by_device_budget(golden):
+    """A request's device footprint (bases, offsets, results and 8 candidates per read) is booked
+    against the server's device budget: one larger than the whole budget is refused for good
+    (MG_ERR_LIMIT); while earlier requests hold the budget a new one waits (MG_ERR_BUSY)."""
+    g = golden("plain")
+    ix = M.Index(g.image)
+    d, o = split(g.reads, [0, 2000])[0]
+    per = len(d) + 8 * (len(o)) + 2000 * (16 + 8 * 16)
+    sv = M.Server(ix, max_inflight_reads=1024, device_budget=int(per * 1.5))
+    with pytest.raises(M.MirageError) as e:
+        sv.submit(*split(g.reads, [0, 4000])[0])
+    assert e.value.code == -4
+    t1 = sv.submit(d, o)
+    assert t1 is not None
+    t2 = None
+    for _ in range(2):  # refused while t1 is booked (unless it has completed already)
+        t2 = sv.submit(d, o)
+        if t2 is None:
+            break
+        sv.wait(t2)
+    same(sv.wait(t1), ix.classify(d, o))
+    t3 = sv.submit(d, o)
+    assert t3 is not None
+    same(sv.wait(t3), ix.classify(d, o))
+    sv.close()
