@@ -153,13 +153,15 @@ int mg_set_probe_slots(mg_index* ix, int on);
 typedef struct {
   uint32_t dual_blocks_per_sm;   /* resident 8-warp blocks per SM of the first dual-strand tier (1-5) */
   uint32_t steal_chunk;          /* reads a warp of that tier takes per work-stealing step (1-64) */
-  uint32_t first_tier;           /* 1: the 64-posting dual-strand tier first (default); 2: reads start at
-                                  * the 128-posting tier (indexes whose strands mostly exceed 64 postings) */
+  uint32_t first_tier;           /* dual-strand tier reads start at: 1 the 64-posting tier (default),
+                                  * 2 the 128-posting one, 3 the 256-posting one (for indexes whose
+                                  * strands mostly exceed the smaller tiers) */
   uint32_t second_blocks_per_sm; /* 4-warp blocks per SM of the 128-posting tier (1-6) */
   uint32_t finish_blocks_per_sm; /* 256-thread blocks per SM of the dual tiers' finishing pass (1-8) */
   uint32_t long_blocks_per_sm;   /* blocks per SM of the long-read tier (1-2) */
   uint32_t chunks;               /* pieces of a large host-buffer batch in mg_classify (1-8) */
   uint32_t weighted_chunks;      /* 1: 8 chunks weighted 1-2-3-3-3-3-2-1; 2: equal chunks */
+  uint32_t third_blocks_per_sm;  /* 2-warp blocks per SM of the 256-posting tier (1-6) */
 } mg_tuning;
 int mg_set_tuning(mg_index* ix, const mg_tuning* t);
 /* The launch shapes in effect (defaults filled in) and the density class used to pick them. */

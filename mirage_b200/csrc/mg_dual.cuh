@@ -24,7 +24,7 @@ namespace mg {
 // Cap entries, at least the distinct references of Cap postings.
 template <int Cap>
 struct alignas(16) DualSmemT {  // 16-byte aligned: the table clear stores 16 bytes a lane
-  static_assert(Cap == 64 || Cap == 128, "postings per strand");
+  static_assert(Cap == 64 || Cap == 128 || Cap == 256, "postings per strand");
   uint32_t a[2][3][Cap];          // gathered postings (ref, pos, found | seed << 8 | table entry << 16);
                                 // from the rank sort on: kept postings sorted (ref, pos, seed)
   uint32_t c[2][3][Cap];          // kept postings, compacted (ref, pos, seed); at the end the run
@@ -145,7 +145,7 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
     const uint32_t i = hl + 16 * s;
     if (i < T) {
       const uint32_t ref = e_ref[i];
-      uint32_t x = (ref * 2654435761u) >> (Cap == 64 ? 26 : 25);  // Cap entries
+      uint32_t x = (ref * 2654435761u) >> (Cap == 64 ? 26 : Cap == 128 ? 25 : 24);  // Cap entries
       for (;;) {
         const uint32_t old = atomicCAS(&tkey[x], EMPTY, ref);
         if (old == EMPTY || old == ref) break;

@@ -332,30 +332,34 @@ __global__ void __launch_bounds__(kFinThreads) k_finish_dual(DevIndex ix, BatchD
   }
 }
 
-// Second dual-strand tier over the first one's leftovers: room for 128 postings per strand (at
-// most 64 of them kept); the reads it takes leave run records for k_finish_dual like the first
-// tier's, its own leftovers go to the general warp tier. 4 warps per block (35 KB of shared memory).
-constexpr int kW2Warps = 4;
-// With all_reads it takes every read of the batch (the first tier is not run).
-__global__ void __launch_bounds__(kW2Warps * 32) k_classify_dual_list(DevIndex ix, BatchDev b, StageDev sd,
-                                                                     int all_reads) {
-  __shared__ DualSmemT<128> sm[kW2Warps];
+// Further dual-strand tiers over the leftovers of the one before: room for Cap postings per
+// strand (128 or 256, at most 64 of them kept); the reads they take leave run records for
+// k_finish_dual like the first tier's, their own leftovers go to the next tier. With all_reads a
+// tier takes every read of the batch (the tiers before it are not run).
+constexpr int kW2Warps = 4;  // warps per block at 128 postings (35 KB of shared memory)
+constexpr int kW3Warps = 2;  // at 256 postings (34 KB)
+template <int Cap, int Warps>
+__global__ void __launch_bounds__(Warps * 32) k_classify_dual_list(DevIndex ix, BatchDev b, StageDev sd,
+                                                                     const uint32_t* list, const unsigned* list_n,
+                                                                     unsigned* cursor, uint32_t* next,
+                                                                     unsigned* next_n, int all_reads) {
+  __shared__ DualSmemT<Cap> sm[Warps];
   __shared__ uint8_t comp[256];
   for (int c = threadIdx.x; c < 256; c += blockDim.x) comp[c] = complement_dev(upper_dev((uint8_t)c));
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  DualSmemT<128>& S = sm[w];
-  const uint32_t n = all_reads ? (uint32_t)b.n : *b.n_ovf0;
+  DualSmemT<Cap>& S = sm[w];
+  const uint32_t n = all_reads ? (uint32_t)b.n : *list_n;
   for (;;) {
     uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(b.work0b, 1u);
+    if (lane == 0) item = atomicAdd(cursor, 1u);
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= n) break;
-    const uint32_t r = all_reads ? item : b.ovf0[item];
+    const uint32_t r = all_reads ? item : list[item];
     if (!process_read_dual(ix, b, r, S, comp, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
       if (lane == 0) {
-        unsigned at = atomicAdd(b.n_ovf0b, 1u);
-        b.ovf0b[at] = r;
+        unsigned at = atomicAdd(next_n, 1u);
+        next[at] = r;
         b.reads[r] = mg_read_result{};  // not kReadUnscored: a later tier writes this read
       }
     }
@@ -967,7 +971,7 @@ static int open_image(mg_index* ix, const uint8_t* image, uint64_t L, int k, int
 // the kernels can be launched with.
 struct Shapes {
   unsigned dual_blocks_per_sm, steal_chunk, first_tier, second_blocks_per_sm, finish_blocks_per_sm,
-      long_blocks_per_sm, chunks, weighted_chunks;
+      long_blocks_per_sm, chunks, weighted_chunks, third_blocks_per_sm;
 };
 
 static int occupancy(const void* fn, int threads, size_t smem) {
@@ -977,10 +981,11 @@ static int occupancy(const void* fn, int threads, size_t smem) {
 }
 
 static Shapes shapes(const mg_index* ix) {
-  static int occ_dual = 0, occ_second = 0, occ_long = 0;
+  static int occ_dual = 0, occ_second = 0, occ_third = 0, occ_long = 0;
   if (!occ_dual) {
     cudaFuncSetAttribute(k_classify_long, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LongSmem));
-    occ_second = occupancy((const void*)k_classify_dual_list, kW2Warps * 32, 0);
+    occ_second = occupancy((const void*)k_classify_dual_list<128, kW2Warps>, kW2Warps * 32, 0);
+    occ_third = occupancy((const void*)k_classify_dual_list<256, kW3Warps>, kW3Warps * 32, 0);
     occ_long = occupancy((const void*)k_classify_long, kLgThreads, sizeof(LongSmem));
     occ_dual = occupancy((const void*)k_classify_dual, kW1Warps * 32, 0);
   }
@@ -989,12 +994,13 @@ static Shapes shapes(const mg_index* ix) {
     return v ? std::min<unsigned>(hi, std::max<unsigned>(lo, v)) : def;
   };
   Shapes s;
-  s.first_tier = pick(t.first_tier, 1, 1, 2);
+  s.first_tier = pick(t.first_tier, 1, 1, 3);
   s.dual_blocks_per_sm = pick(t.dual_blocks_per_sm, (unsigned)occ_dual, 1, (unsigned)occ_dual);
   s.steal_chunk = pick(t.steal_chunk, kW1Chunk, 1, 64);
   // the 128-posting tier takes the first tier's few leftovers (one block per SM), or every read
   s.second_blocks_per_sm = pick(t.second_blocks_per_sm, s.first_tier == 2 ? (unsigned)occ_second : 1u, 1,
                                 (unsigned)occ_second);
+  s.third_blocks_per_sm = pick(t.third_blocks_per_sm, (unsigned)occ_third, 1, (unsigned)occ_third);
   s.finish_blocks_per_sm = pick(t.finish_blocks_per_sm, 8, 1, 8);
   s.long_blocks_per_sm = pick(t.long_blocks_per_sm, (unsigned)occ_long, 1, (unsigned)occ_long);
   s.chunks = pick(t.chunks, mg_index::kMaxChunks, 1, mg_index::kMaxChunks);
@@ -1056,6 +1062,7 @@ static void load_tuning(mg_index* ix) {
       else if (k == "long_blocks_per_sm") t.long_blocks_per_sm = v;
       else if (k == "chunks") t.chunks = v;
       else if (k == "weighted_chunks") t.weighted_chunks = v;
+      else if (k == "third_blocks_per_sm") t.third_blocks_per_sm = v;
     }
   }
 }
@@ -1069,7 +1076,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
   }
   if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
       w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
-      w.ovf.alloc(5 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+      w.ovf.alloc(6 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
@@ -1078,7 +1085,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
 // 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovf0b | 60 work0b |
-// 64 n_ovf1b | 68 work of the long-read tier
+// 64 n_ovf1b | 68 work of the long-read tier | 72 n_ovf0c | 76 work0c
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
                         bool plain, unsigned long long* chain, const ChainSync* cs) {
@@ -1109,6 +1116,9 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   uint32_t* ovf1b = w.ovf.as<uint32_t>() + 4 * (n + 4);  // the long-read tier's leftovers
   unsigned* n_ovf1b = (unsigned*)(ctr + 64);
   unsigned* work_long = (unsigned*)(ctr + 68);
+  uint32_t* ovf0c = w.ovf.as<uint32_t>() + 5 * (n + 4);  // the 128-posting tier's leftovers
+  unsigned* n_ovf0c = (unsigned*)(ctr + 72);
+  unsigned* work0c = (unsigned*)(ctr + 76);
   StageDev sd;
   sd.stage = w.stage.as<mg_candidate>();
   sd.arena = w.arena.as<mg_candidate>();
@@ -1155,8 +1165,12 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       const Shapes sh = shapes(ix);
       if (sh.first_tier == 1)
         k_classify_dual<<<sh.dual_blocks_per_sm * sms, kW1Warps * 32, 0, st>>>(ix->dix, b, sd, sh.steal_chunk);
-      k_classify_dual_list<<<sh.second_blocks_per_sm * sms, kW2Warps * 32, 0, st>>>(ix->dix, b, sd,
-                                                                                     sh.first_tier == 2);
+      // tiers of 64, 128 and 256 postings per strand, each over the one before's leftovers
+      if (sh.first_tier <= 2)
+        k_classify_dual_list<128, kW2Warps><<<sh.second_blocks_per_sm * sms, kW2Warps * 32, 0, st>>>(
+            ix->dix, b, sd, b.ovf0, b.n_ovf0, b.work0b, ovf0c, n_ovf0c, sh.first_tier == 2);
+      k_classify_dual_list<256, kW3Warps><<<sh.third_blocks_per_sm * sms, kW3Warps * 32, 0, st>>>(
+          ix->dix, b, sd, ovf0c, n_ovf0c, work0c, b.ovf0b, b.n_ovf0b, sh.first_tier == 3);
       // the reads the dual tiers handed on go through the other tiers on the side stream, beside
       // the dual tier's finishing pass (different reads, disjoint slots; arena space by atomics)
       CU(cudaEventRecord(w.fork, st));
@@ -1538,7 +1552,7 @@ int mg_get_tuning(const mg_index* ix, mg_tuning* t, char* cls, uint64_t cls_len)
   CU(cudaSetDevice(ix->device));
   const Shapes s = shapes(ix);
   *t = mg_tuning{s.dual_blocks_per_sm, s.steal_chunk, s.first_tier, s.second_blocks_per_sm,
-                 s.finish_blocks_per_sm, s.long_blocks_per_sm, s.chunks, s.weighted_chunks};
+                 s.finish_blocks_per_sm, s.long_blocks_per_sm, s.chunks, s.weighted_chunks, s.third_blocks_per_sm};
   if (cls && cls_len) std::snprintf(cls, cls_len, "%s", density_class(ix->info.n_postings));
   return MG_OK;
 }

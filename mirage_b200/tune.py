@@ -31,10 +31,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 # fields and candidate values, in the order they are swept
 SHORT_GRID = {
-    "first_tier": [1, 2],
+    "first_tier": [1, 2, 3],
     "dual_blocks_per_sm": [3, 4, 5],
     "steal_chunk": [1, 2, 4, 8, 16],
     "second_blocks_per_sm": [1, 2, 4, 6],
+    "third_blocks_per_sm": [2, 4, 6],
     "finish_blocks_per_sm": [2, 4, 8],
 }
 LONG_GRID = {"long_blocks_per_sm": [1, 2]}

@@ -270,3 +270,48 @@ def test_long_read_tier_and_its_hand_offs(tmp_path):
         seqs.append(r.tobytes().lower())
     seqs.append(refs[4][1000:9000].tobytes())
     check_against_oracle(gix, oix, seqs)
+
+
+@pytest.mark.parametrize("first_tier", [1, 2, 3])
+def test_strands_of_129_to_256_postings(tmp_path, first_tier):
+    """Reads whose forward strand gathers 160 postings, 40 of them kept: five copies of the
+    reference the reads come from and thirty decoys holding every other seed window of each read
+    (never kept). Such strands pass the 64- and 128-posting dual-strand tiers on to the 256-posting
+    one; with first_tier 2 or 3 the reads start at the larger tiers. Every setting equals the
+    oracle, and the three settings agree bit for bit."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(37)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 20000)]
+    k, step, hlen, L = 31, 15, 17, 150
+    starts = np.arange(100) * 200
+    seqs = [core[s:s + L].tobytes() for s in starts]
+    ns = (L - k + step - 1) // step
+    decoys = []
+    for _ in range(30):
+        parts = []
+        for s in starts:
+            for j in range(0, ns, 2):
+                parts.append(core[s + j * step:s + j * step + hlen])
+                parts.append(acgt[rng.integers(0, 4, 20)])
+        decoys.append(np.concatenate(parts))
+    refs = [core] * 5 + decoys
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    key = "decoys30"
+    if key not in _ix:
+        image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))], k=k)
+        path = tmp_path / "decoys30.mhm"
+        image.tofile(path)
+        _ix[key] = (M.Index(image, k=k), O.Index(str(path), k=k))
+    gix, oix = _ix[key]
+    hashes = [O.lib().mgo_hash28(q[j * step:j * step + hlen], hlen) for q in seqs for j in range(ns)]
+    per_read = gix.bucket_sizes(np.array(hashes, np.uint32)).astype(np.int64).reshape(len(seqs), ns).sum(1)
+    assert (per_read > 128).all() and (per_read <= 256).all(), per_read
+    gix.set_tuning(first_tier=first_tier)
+    try:
+        r = check_against_oracle(gix, oix, seqs)
+    finally:
+        gix.set_tuning()
+    assert (r.reads["n_fwd"] >= 5).all()
