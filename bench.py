@@ -358,12 +358,13 @@ def run_reference_arm(args, rank: int, world: int) -> None:
 
 
 def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s: float, clients: int = 8,
-                 fracs=(0.25, 0.5, 0.75, 0.9)):
+                 fracs=(0.25, 0.5, 0.75, 0.9, 1.0, 1.1)):
     """Served form (mg_server_*): saturated throughput, then latency under Poisson arrivals at
     fractions of it. Native client threads (mirage_b200/libmg_loadgen.so) drive the server
     through the public C ABI: requests are contiguous slices of the host reads with log-uniform
-    sizes in [1, 50000] reads, each submit copies its request from host memory and each wait
-    copies its results into the client's buffers, inside the measurement."""
+    sizes in [1, 50000] reads; each submit copies its request from host memory and the server
+    writes its results into the client's own buffers (mg_server_submit_into), inside the
+    measurement."""
     import ctypes as C
 
     class Report(C.Structure):
@@ -388,7 +389,7 @@ def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s:
 
     try:
         run(0.0, 0.5, 32, 0)  # warm-up
-        sat = run(0.0, level_s, 32, 1)
+        sat = run(0.0, min(level_s, 5.0), 32, 1)
         levels = []
         for i, f in enumerate(fracs):
             r = run(f * sat.reads_per_s, level_s, 1, 2 + i)
@@ -397,6 +398,7 @@ def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s:
         return {"saturated": {"value": sat.reads_per_s, "unit": "reads/s", "p50_ms": sat.p50_ms, "p99_ms": sat.p99_ms},
                 "requests": "log-uniform 1..50000 reads, contiguous slices of the batch",
                 "clients": f"{clients} native threads (libmg_loadgen.so), closed loop 32 deep when saturated",
+                "results": "written by the server into each client's buffers (mg_server_submit_into)",
                 "arrivals": "Poisson (one process per client thread)", "seconds_per_level": level_s, "load": levels}
     finally:
         sv.close()
@@ -416,7 +418,7 @@ def main():
     ap.add_argument("--reads", type=int, default=None, help="reads per GPU per step (default: the workload's)")
     ap.add_argument("--cpu-sample", type=int, default=None, help="reads of the CPU baseline and parity sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--served-seconds", type=float, default=3.0, help="seconds per served-form load level (0: skip)")
+    ap.add_argument("--served-seconds", type=float, default=10.0, help="seconds per served-form load level (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.reads is None:
