@@ -17,6 +17,7 @@
 #include <fstream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -168,7 +169,12 @@ int main(int argc, char** argv) {
   const std::string speed = lower(cfg.get("UltraFastMode", "sensitive"));
   const std::string mem = lower(cfg.get("Hashmap_Load_Reference_Memory_UsageMode", "extreme"));
   const bool save_db = cfg.get("output_save_hashmap_database", "1") != "0";
-  const uint64_t batch = std::max<uint64_t>(1000000, std::strtoull(cfg.get("Hardware_BlockSize_Default_GPU", "20000").c_str(), nullptr, 10));
+  // reads per mg_classify call: GPU_BatchReads (this program's own key) when given, else the
+  // reference's GPU block size raised to at least 1,000,000 (the batched form's efficient size)
+  const std::string gb = cfg.get("GPU_BatchReads", "");
+  const uint64_t batch =
+      gb.empty() ? std::max<uint64_t>(1000000, std::strtoull(cfg.get("Hardware_BlockSize_Default_GPU", "20000").c_str(), nullptr, 10))
+                 : std::max<uint64_t>(1, std::strtoull(gb.c_str(), nullptr, 10));
   if (speed != "sensitive") {
     std::fprintf(stderr, "mirage_gpu: UltraFastMode '%s' is not supported (only Sensitive).\n", speed.c_str());
     return 1;
@@ -237,36 +243,52 @@ int main(int argc, char** argv) {
   const uint64_t n = q.headers.size();
   auto t1 = std::chrono::steady_clock::now();
   uint64_t reported = 0;
-  std::vector<mg_read_result> reads;
-  std::vector<mg_candidate> cands;
-  std::vector<uint64_t> offs, ids;
-  std::vector<const char*> in_headers;
-  for (uint64_t b0 = 0; b0 < n; b0 += batch) {
+  // Two result buffers: batch i+1 is classified into one while a writer thread logs batch i from
+  // the other (LogMatrixResults / LogResultsToFileManager, Analyser.cpp:228-491, run off the
+  // GPU's critical path). Batches are logged in order, one at a time.
+  struct Buf {
+    std::vector<mg_read_result> reads;
+    std::vector<mg_candidate> cands;
+    std::vector<uint64_t> offs, ids;
+    std::vector<const char*> in_headers;
+    uint64_t m = 0;
+  } buf[2];
+  std::thread writer;
+  int write_rc = 0;
+  uint64_t bi = 0;
+  for (uint64_t b0 = 0; b0 < n; b0 += batch, bi++) {
+    Buf& B = buf[bi & 1];  // last logged two batches ago; that writer was joined one batch ago
     const uint64_t b1 = std::min(n, b0 + batch), m = b1 - b0;
-    offs.assign(m + 1, 0);
-    for (uint64_t i = 0; i <= m; i++) offs[i] = q.offs[b0 + i] - q.offs[b0];
-    reads.assign(m, mg_read_result{});
-    cands.resize(std::max<uint64_t>(cands.size(), 8 * m + 1024));
-    mg_batch bt{m, offs.data(), q.bases.data() + q.offs[b0]};
-    mg_result res{reads.data(), cands.data(), cands.size(), 0};
+    B.m = m;
+    B.offs.assign(m + 1, 0);
+    for (uint64_t i = 0; i <= m; i++) B.offs[i] = q.offs[b0 + i] - q.offs[b0];
+    B.reads.assign(m, mg_read_result{});
+    B.cands.resize(std::max<uint64_t>(B.cands.size(), 8 * m + 1024));
+    mg_batch bt{m, B.offs.data(), q.bases.data() + q.offs[b0]};
+    mg_result res{B.reads.data(), B.cands.data(), B.cands.size(), 0};
     rc = mg_classify(ix, &bt, &res);
-    if (rc == MG_ERR_OOM && res.n_cands > cands.size()) {
-      cands.resize(res.n_cands);
-      res = mg_result{reads.data(), cands.data(), cands.size(), 0};
+    if (rc == MG_ERR_OOM && res.n_cands > B.cands.size()) {
+      B.cands.resize(res.n_cands);
+      res = mg_result{B.reads.data(), B.cands.data(), B.cands.size(), 0};
       rc = mg_classify(ix, &bt, &res);
     }
     if (rc) die("classifying", rc);
-    ids.resize(m);
-    in_headers.resize(m);
+    B.ids.resize(m);
+    B.in_headers.resize(m);
     for (uint64_t i = 0; i < m; i++) {
-      ids[i] = b0 + i;
-      in_headers[i] = q.headers[b0 + i].c_str();
-      reported += reads[i].reported;
+      B.ids[i] = b0 + i;
+      B.in_headers[i] = q.headers[b0 + i].c_str();
+      reported += B.reads[i].reported;
     }
-    rc = mg_logs_write(logs, reads.data(), cands.data(), m, ids.data(), in_headers.data(), ref_headers.data(),
-                       taxids.data(), first_only ? 1 : 0);
-    if (rc) die("writing the result logs", rc);
+    if (writer.joinable()) writer.join();
+    if (write_rc) die("writing the result logs", write_rc);
+    writer = std::thread([&, bp = &B] {
+      write_rc = mg_logs_write(logs, bp->reads.data(), bp->cands.data(), bp->m, bp->ids.data(), bp->in_headers.data(),
+                               ref_headers.data(), taxids.data(), first_only ? 1 : 0);
+    });
   }
+  if (writer.joinable()) writer.join();
+  if (write_rc) die("writing the result logs", write_rc);
   mg_logs_close(logs);
   auto t2 = std::chrono::steady_clock::now();
   const double a = std::chrono::duration<double>(t2 - t1).count(), all = std::chrono::duration<double>(t2 - t0).count();

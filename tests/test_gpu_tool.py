@@ -60,3 +60,8 @@ def test_tool_from_fasta_and_from_mhm(golden, tmp_path):
     d2 = run_tool(tmp, CFG.format(query="/nonexistent", reference=refs, out=os.path.join(tmp, "out")),
                   "-reference", saved, "-input", reads)
     assert open(os.path.join(d2, "results_Raw.log"), "rb").read() == exp
+    # batches of 1,500 reads: each batch's logs are written by a thread while the next batch is
+    # classified; the log is the same, in the same order
+    time.sleep(1.1)
+    d3 = run_tool(tmp, CFG.format(query=reads, reference=saved, out=os.path.join(tmp, "out")), "-GPU_BatchReads", "1500")
+    assert open(os.path.join(d3, "results_Raw.log"), "rb").read() == exp
