@@ -59,7 +59,8 @@ __device__ __forceinline__ bool lg_contains(const uint32_t* set, uint32_t mask, 
   }
 }
 
-// Inserts key; true when this call inserted it (false: it was there already).
+// Inserts key; true when this call inserted it (false: it was there already). Every caller keeps
+// its table at most half full, so an empty slot is always found.
 __device__ __forceinline__ bool lg_insert(uint32_t* set, uint32_t mask, uint32_t key) {
   for (uint32_t s = lg_mix(key) & mask;; s = (s + 1) & mask) {
     const uint32_t old = atomicCAS(&set[s], kLgEmpty, key);
@@ -183,8 +184,13 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
   // reach a diagonal run of 2 either, so the strand has no candidate
   if (hs < 2) return kStrandOk;
   const uint32_t keep_min = hs - 1;  // max(1, hs - 1), Analyser.cpp:2115
+  // each insertion attempt first claims a count (n_rt, an upper bound of the distinct references:
+  // threads racing on one reference each claim one): at most kLgRT / 2 insertions happen, so the
+  // table never fills, and a refused one leaves n_rt above kLgRT / 2, which sends the strand to the
+  // block tier
   for (uint32_t i = tid; i < ne; i += G)
-    if (run_from(i) >= keep_min && lg_insert(S.rt, kLgRT - 1, S.p_ref[i])) atomicAdd(&S.n_rt, 1u);
+    if (run_from(i) >= keep_min && !lg_contains(S.rt, kLgRT - 1, S.p_ref[i]))
+      if (atomicAdd(&S.n_rt, 1u) < (uint32_t)kLgRT / 2) lg_insert(S.rt, kLgRT - 1, S.p_ref[i]);
   __syncthreads();
   if (S.n_rt > (uint32_t)kLgRT / 2) return kStrandOverflow;
   // 3. the kept references' postings, as (refID << 32 | position, query position) sort keys

@@ -315,3 +315,26 @@ def test_strands_of_129_to_256_postings(tmp_path, first_tier):
     finally:
         gix.set_tuning()
     assert (r.reads["n_fwd"] >= 5).all()
+
+
+def test_long_reads_with_more_kept_references_than_the_long_tier_holds(tmp_path):
+    """Reads of 450-600 bases on 130 identical references: about 3,600 postings per strand, every
+    reference kept, more than the long-read tier's table of kept references takes (64), so the
+    reads go on to the block tier and, beyond its 128 candidates, to the global tier; the results
+    equal the oracle."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(47)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 5000)]
+    refs = [core] * 130 + [acgt[rng.integers(0, 4, 5000)]]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))])
+    path = tmp_path / "many.mhm"
+    image.tofile(path)
+    gix = M.Index(image)
+    oix = O.Index(str(path))
+    seqs = [core[s:s + n].tobytes() for s, n in zip(rng.integers(0, 4000, 6), (450, 480, 500, 530, 560, 600))]
+    r = check_against_oracle(gix, oix, seqs)
+    assert (r.reads["n_fwd"] + r.reads["n_rc"] >= 130).all()
