@@ -527,6 +527,27 @@ def main():
         total_ms = max_over_ranks(total_ms)
         ms_per_step = total_ms / args.steps
         value = world * n / (ms_per_step / 1000)
+        # the launch shapes in effect (the tuning file's, for this GPU model and index class),
+        # and the same device step under the library's defaults, untimed by the line's value
+        shapes, density = ix.get_tuning()
+        ix.set_tuning()
+        defaults = ix.get_tuning()[0]
+        default_ms = None
+        if defaults != shapes:
+            ts = []
+            for i in range(3 + min(args.steps, 10)):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                device_step()
+                e1.record(stream)
+                ix.device_sync(sp)
+                if i >= 3:
+                    ts.append(e0.elapsed_time(e1))
+            default_ms = float(np.mean(ts))
+        ix.set_tuning(**shapes)
+        tuning = {"density_class": density, "shapes": shapes, "source": os.environ.get("MG_TUNING_FILE") or
+                  "tuning file of this GPU model beside the library (defaults where it has no entry)",
+                  "ms_per_step": ms_per_step, "defaults": defaults, "default_ms_per_step": default_ms or ms_per_step}
 
         # end to end through the C ABI with pinned host buffers
         for _ in range(args.warmup):
@@ -629,6 +650,7 @@ def main():
                                        "compaction": kernel_ms[4] / args.steps},
                 "roofline": roof, "cpu_baseline": cpu, "parity": parity, "clocks": clk.summary(),
                 "gpu_launches": args.steps * LAUNCHES_PER_BATCH,
+                "tuning": tuning,
                 "setup_s": {"generate": t_gen, "index_build_device": t_build, "open": t_open}}
         print(json.dumps(line), flush=True)
     ix.close()
