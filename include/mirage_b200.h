@@ -162,6 +162,9 @@ typedef struct {
   uint32_t chunks;               /* pieces of a large host-buffer batch in mg_classify (1-8) */
   uint32_t weighted_chunks;      /* 1: 8 chunks weighted 1-2-3-3-3-3-2-1; 2: equal chunks */
   uint32_t third_blocks_per_sm;  /* 2-warp blocks per SM of the 256-posting tier (1-6) */
+  uint32_t pack_bases;           /* mg_classify's upload of the bases: 1 as given (default); 2 packed 2 bits
+                                  * per base on host threads (other bytes as a list of exceptions) and
+                                  * unpacked on the device, a quarter of the bytes over the link */
 } mg_tuning;
 int mg_set_tuning(mg_index* ix, const mg_tuning* t);
 /* The launch shapes in effect (defaults filled in) and the density class used to pick them. */

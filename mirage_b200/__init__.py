@@ -58,7 +58,7 @@ class _Info(C.Structure):
 
 
 TUNING_FIELDS = ("dual_blocks_per_sm", "steal_chunk", "first_tier", "second_blocks_per_sm", "finish_blocks_per_sm",
-                 "long_blocks_per_sm", "chunks", "weighted_chunks", "third_blocks_per_sm")
+                 "long_blocks_per_sm", "chunks", "weighted_chunks", "third_blocks_per_sm", "pack_bases")
 
 
 class _Tuning(C.Structure):

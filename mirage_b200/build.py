@@ -21,8 +21,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2,-fno-fast-math",
           "-Xcompiler", "-ffp-contract=off"]
 
-LIB_SOURCES = ["mg_lib.cu", "mg_server.cu", "mhm.cpp", "mg_output.cu", "mg_noalloc.cu", "mg_build.cu", "mg_parse.cu"]
-HEADERS = ["mg_device.cuh", "mg_kernels.cuh", "mg_lean.cuh", "mg_dual.cuh", "mhm.h", "mg_internal.h", "mg_ring.h"]
+LIB_SOURCES = ["mg_lib.cu", "mg_server.cu", "mhm.cpp", "mg_output.cu", "mg_noalloc.cu", "mg_build.cu", "mg_parse.cu",
+               "mg_pack.cpp"]
+HEADERS = ["mg_device.cuh", "mg_kernels.cuh", "mg_lean.cuh", "mg_dual.cuh", "mg_long.cuh", "mhm.h", "mg_internal.h",
+           "mg_ring.h", "mg_pack.h"]
 TOOL_SOURCES = ["mirage_gpu.cpp"]
 LOADGEN_SOURCES = ["mg_loadgen.cpp"]
 

@@ -9,6 +9,7 @@
 
 #include "../../include/mirage_b200.h"
 #include "mg_device.cuh"
+#include "mg_pack.h"
 #include "mhm.h"
 
 namespace mg {
@@ -39,12 +40,14 @@ struct DevBuf {
 // Device buffers of one classification call in flight (a call owns one at a time).
 struct Workspace {
   DevBuf offs, bases, reads, stage, arena, cands, ctr, ovf, sums, gws, chain;
+  DevBuf packed, exc;  // 2-bit packed bases and their exceptions (mg_classify with pack_bases)
   // the stream on which the tiers after the dual tier run beside its finishing pass, and the
   // events that fork it from and join it back to the call's stream (made at first use)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   void release() {
-    for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws, &chain}) b->release();
+    for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws, &chain, &packed, &exc})
+      b->release();
     if (side) cudaStreamDestroy(side);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
@@ -52,7 +55,8 @@ struct Workspace {
     fork = join = nullptr;
   }
   size_t bytes() const {
-    return offs.n + bases.n + reads.n + stage.n + arena.n + cands.n + ctr.n + ovf.n + sums.n + gws.n + chain.n;
+    return offs.n + bases.n + reads.n + stage.n + arena.n + cands.n + ctr.n + ovf.n + sums.n + gws.n + chain.n +
+           packed.n + exc.n;
   }
 };
 
@@ -110,6 +114,12 @@ struct mg_index {
   std::mutex mu;
   std::atomic<int> n_servers{0};  // mg_server objects attached to this index
   mg_tuning tune{};               // launch shapes (mg_set_tuning); zero fields: defaults
+  // 2-bit packing of the uploaded bases (mg_classify): host threads and pinned staging
+  mg::PackPool* pack_pool = nullptr;
+  uint8_t* h_pack = nullptr;
+  uint64_t h_pack_cap = 0;
+  uint64_t* h_exc = nullptr;
+  uint64_t h_exc_cap = 0;
   mg_index_info info{};
   uint64_t device_bytes = 0;
   // optional per-kernel timing of the last pipeline (events on the launching stream)

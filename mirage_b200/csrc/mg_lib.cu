@@ -458,6 +458,26 @@ __global__ void __launch_bounds__(G) k_classify_block(DevIndex ix, BatchDev b, S
   }
 }
 
+// 2-bit packed bases (mg_pack.cpp) back to ASCII: byte i of packed holds bases 4i..4i+3, the first
+// in the low bits, codes 0-3 for A, C, G, T; then the listed exception bytes at their offsets.
+__global__ void k_unpack_bases(const uint8_t* packed, uint64_t n, uint8_t* out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n + 3) / 4; i += stride) {
+    const uint32_t v = packed[i];
+#pragma unroll
+    for (int t = 0; t < 4; t++)
+      if (4 * i + t < n) out[4 * i + t] = (uint8_t)(0x54474341u >> (8 * ((v >> (2 * t)) & 3u)));  // "ACGT"
+  }
+}
+
+__global__ void k_unpack_exceptions(const uint64_t* exc, uint64_t n_exc, uint64_t n, uint8_t* out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n_exc; j += stride) {
+    const uint64_t e = exc[j];
+    if ((e >> 8) < n) out[e >> 8] = (uint8_t)(e & 0xFFu);
+  }
+}
+
 // Output compaction: exclusive scan of per-read candidate counts, then a scatter into one
 // contiguous array in read order.
 constexpr int kScanBlock = 1024;
@@ -971,7 +991,7 @@ static int open_image(mg_index* ix, const uint8_t* image, uint64_t L, int k, int
 // the kernels can be launched with.
 struct Shapes {
   unsigned dual_blocks_per_sm, steal_chunk, first_tier, second_blocks_per_sm, finish_blocks_per_sm,
-      long_blocks_per_sm, chunks, weighted_chunks, third_blocks_per_sm;
+      long_blocks_per_sm, chunks, weighted_chunks, third_blocks_per_sm, pack_bases;
 };
 
 static int occupancy(const void* fn, int threads, size_t smem) {
@@ -1001,6 +1021,7 @@ static Shapes shapes(const mg_index* ix) {
   s.second_blocks_per_sm = pick(t.second_blocks_per_sm, s.first_tier == 2 ? (unsigned)occ_second : 1u, 1,
                                 (unsigned)occ_second);
   s.third_blocks_per_sm = pick(t.third_blocks_per_sm, (unsigned)occ_third, 1, (unsigned)occ_third);
+  s.pack_bases = pick(t.pack_bases, 1, 1, 2);
   s.finish_blocks_per_sm = pick(t.finish_blocks_per_sm, 8, 1, 8);
   s.long_blocks_per_sm = pick(t.long_blocks_per_sm, (unsigned)occ_long, 1, (unsigned)occ_long);
   s.chunks = pick(t.chunks, mg_index::kMaxChunks, 1, mg_index::kMaxChunks);
@@ -1063,6 +1084,7 @@ static void load_tuning(mg_index* ix) {
       else if (k == "chunks") t.chunks = v;
       else if (k == "weighted_chunks") t.weighted_chunks = v;
       else if (k == "third_blocks_per_sm") t.third_blocks_per_sm = v;
+      else if (k == "pack_bases") t.pack_bases = v;
     }
   }
 }
@@ -1304,6 +1326,31 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   Workspace* cws[2] = {&w, &ix->ws2};
   unsigned long long* chain = w.chain.as<unsigned long long>();
   CU(cudaMemsetAsync(chain, 0, 16, ix->h2d));
+  // packed upload: pinned staging for every chunk's packed bases and exceptions (a chunk with more
+  // exceptions than its share goes up as given)
+  const bool pack = sh.pack_bases == 2;
+  const uint64_t n_bases = batch->offsets[n];
+  const uint64_t pack_need = n_bases / 4 + 64 * (uint64_t)(nc + 1), exc_need = n_bases / 32 + 4096 * (uint64_t)nc;
+  if (pack) {
+    if (!ix->pack_pool)
+      ix->pack_pool = new PackPool((int)std::min(16u, std::max(1u, std::thread::hardware_concurrency())));
+    if (ix->h_pack_cap < pack_need) {
+      if (ix->h_pack) cudaFreeHost(ix->h_pack);
+      ix->h_pack = nullptr;
+      ix->h_pack_cap = 0;
+      CU(cudaMallocHost((void**)&ix->h_pack, pack_need));
+      ix->h_pack_cap = pack_need;
+    }
+    if (ix->h_exc_cap < exc_need) {
+      if (ix->h_exc) cudaFreeHost(ix->h_exc);
+      ix->h_exc = nullptr;
+      ix->h_exc_cap = 0;
+      CU(cudaMallocHost((void**)&ix->h_exc, exc_need * 8));
+      ix->h_exc_cap = exc_need;
+    }
+    if (w.packed.alloc(pack_need) || w.exc.alloc(exc_need * 8)) return set_error(MG_ERR_OOM, "packed staging");
+  }
+  uint64_t pk = 0, ek = 0;  // staging offsets of the next chunk's packed bytes and exceptions
   for (int i = 0; i < nc && rc == MG_OK; i++) {
     const uint64_t r0 = bound[i], r1 = bound[i + 1];
     const uint64_t b0 = batch->offsets[r0], b1 = batch->offsets[r1];
@@ -1311,10 +1358,35 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
     // each chunk's offsets travel with its bases (the shared boundary entry twice, same value)
     CU(cudaMemcpyAsync(w.offs.as<uint64_t>() + r0, batch->offsets + r0, (r1 - r0 + 1) * 8, cudaMemcpyHostToDevice,
                        ix->h2d));
-    if (b1 > b0)
+    bool packed = false;
+    uint64_t n_exc = 0;
+    const uint64_t pb = (b1 - b0 + 3) / 4;
+    if (pack && b1 > b0) {
+      // packed on the host while the device works on the earlier chunks
+      const uint64_t cap = (exc_need - ek) / (uint64_t)(nc - i);
+      pack_bases(*ix->pack_pool, batch->bases + b0, b1 - b0, ix->h_pack + pk, ix->h_exc + ek, cap, &n_exc);
+      packed = n_exc <= cap;
+    }
+    if (packed) {
+      CU(cudaMemcpyAsync(w.packed.as<uint8_t>() + pk, ix->h_pack + pk, pb, cudaMemcpyHostToDevice, ix->h2d));
+      if (n_exc)
+        CU(cudaMemcpyAsync(w.exc.as<uint64_t>() + ek, ix->h_exc + ek, n_exc * 8, cudaMemcpyHostToDevice, ix->h2d));
+    } else if (b1 > b0) {
       CU(cudaMemcpyAsync(w.bases.as<uint8_t>() + b0, batch->bases + b0, b1 - b0, cudaMemcpyHostToDevice, ix->h2d));
+    }
     CU(cudaEventRecord(ix->ev_in[i], ix->h2d));
     CU(cudaStreamWaitEvent(st, ix->ev_in[i], 0));
+    if (packed) {
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device);
+      k_unpack_bases<<<(unsigned)sms * 4, 256, 0, st>>>(w.packed.as<uint8_t>() + pk, b1 - b0, w.bases.as<uint8_t>() + b0);
+      if (n_exc)
+        k_unpack_exceptions<<<(unsigned)std::min<uint64_t>((n_exc + 255) / 256, (uint64_t)sms * 4), 256, 0, st>>>(
+            w.exc.as<uint64_t>() + ek, n_exc, b1 - b0, w.bases.as<uint8_t>() + b0);
+      CU(cudaGetLastError());
+      pk += (pb + 15) / 16 * 16;
+      ek += n_exc;
+    }
     const ChainSync cs{i ? ix->ev_scan[i - 1] : nullptr, ix->ev_scan[i], ix->h_snap + i};
     rc = run_pipeline(ix, *cws[i & 1], r1 - r0, w.offs.as<uint64_t>() + r0, w.bases.as<uint8_t>(),
                       w.reads.as<mg_read_result>() + r0, w.cands.as<mg_candidate>(), out->cand_cap, st, false, chain,
@@ -1479,6 +1551,9 @@ void mg_close(mg_index* ix) {
     }
     cudaFreeHost(ix->h_snap);
   }
+  delete ix->pack_pool;
+  if (ix->h_pack) cudaFreeHost(ix->h_pack);
+  if (ix->h_exc) cudaFreeHost(ix->h_exc);
   delete ix;
 }
 
@@ -1552,7 +1627,8 @@ int mg_get_tuning(const mg_index* ix, mg_tuning* t, char* cls, uint64_t cls_len)
   CU(cudaSetDevice(ix->device));
   const Shapes s = shapes(ix);
   *t = mg_tuning{s.dual_blocks_per_sm, s.steal_chunk, s.first_tier, s.second_blocks_per_sm,
-                 s.finish_blocks_per_sm, s.long_blocks_per_sm, s.chunks, s.weighted_chunks, s.third_blocks_per_sm};
+                 s.finish_blocks_per_sm, s.long_blocks_per_sm, s.chunks, s.weighted_chunks, s.third_blocks_per_sm,
+                 s.pack_bases};
   if (cls && cls_len) std::snprintf(cls, cls_len, "%s", density_class(ix->info.n_postings));
   return MG_OK;
 }

@@ -338,3 +338,34 @@ def test_long_reads_with_more_kept_references_than_the_long_tier_holds(tmp_path)
     seqs = [core[s:s + n].tobytes() for s, n in zip(rng.integers(0, 4000, 6), (450, 480, 500, 530, 560, 600))]
     r = check_against_oracle(gix, oix, seqs)
     assert (r.reads["n_fwd"] + r.reads["n_rc"] >= 130).all()
+
+
+def test_packed_upload_equals_plain_upload(golden):
+    """mg_classify with pack_bases = 2 (bases packed 2 bits each on host threads, other bytes sent
+    as exceptions, unpacked on the device) gives the same bytes as the upload of the bases as
+    given: on 165,000 reads in chunks, with lowercase bases, N and IUPAC bytes scattered, and one
+    stretch of reads of N only (more exceptions than a chunk's share: that chunk goes up as given);
+    a byte without a reverse complement still fails the call."""
+    g = golden("uneven_small")
+    ix = M.Index(g.image)
+    data, offs = _tile(g.reads.data, g.reads.offs, 55)
+    data = data.copy()
+    rng = np.random.default_rng(53)
+    low = rng.random(len(data)) < 0.05
+    data[low] = data[low] | 0x20
+    for c in b"NRYSWKMBDHV":
+        data[rng.integers(0, len(data), 200)] = c
+    a, b = int(offs[40000]), int(offs[46000])  # 6,000 reads of N only
+    data[a:b] = ord("N")
+    want = ix.classify(data, offs)
+    ix.set_tuning(pack_bases=2)
+    try:
+        got = ix.classify(data, offs)
+        _same(want, got)
+        bad = data.copy()
+        bad[int(offs[120000]) + 5] = ord("X")
+        with pytest.raises(M.MirageError) as e:
+            ix.classify(bad, offs)
+        assert e.value.code == -6
+    finally:
+        ix.set_tuning()
