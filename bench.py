@@ -559,7 +559,26 @@ def main():
         torch.cuda.synchronize()
         e2e_s = max_over_ranks(time.perf_counter() - t) / args.steps
         e2e = world * n / e2e_s
-    h2d = n_bases + 8 * (n + 1)
+        # the same e2e measurement with the other upload of the bases (packed 2 bits per base on
+        # host threads and unpacked on the device, or copied as given)
+        upload = shapes["pack_bases"]
+        ix.set_tuning(**{**shapes, "pack_bases": 3 - upload})
+        for _ in range(2):
+            e2e_step()
+        barrier()
+        k2 = max(1, min(args.steps, 10))
+        t = time.perf_counter()
+        for _ in range(k2):
+            e2e_step()
+        torch.cuda.synchronize()
+        other_s = max_over_ranks(time.perf_counter() - t) / k2
+        ix.set_tuning(**shapes)
+    acgt = np.zeros(256, bool)
+    acgt[list(b"ACGTacgt")] = True
+    n_exc = int((~acgt[reads.data]).sum())
+    h2d_given = n_bases + 8 * (n + 1)
+    h2d_packed = (n_bases + 3) // 4 + 8 * n_exc + 8 * (n + 1)
+    h2d = h2d_packed if upload == 2 else h2d_given
     d2h = 16 * n + 16 * n_c + 64
     link_gbs = h2d_link_gbs(h_bases, d_bases)
 
@@ -633,6 +652,12 @@ def main():
                            "parallelism": f"replicas x{world}, reads sharded"},
                 "e2e": {"value": e2e, "unit": "reads/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": 1000 * e2e_s, "host_buffers": "pinned",
+                        "upload": "bases packed 2 bits each on host threads, unpacked on the device" if upload == 2
+                                  else "bases copied as given",
+                        "other_upload": {"upload": "bases copied as given" if upload == 2 else
+                                         "bases packed 2 bits each on host threads, unpacked on the device",
+                                         "value": world * n / other_s, "ms_per_step": 1000 * other_s,
+                                         "h2d_bytes_per_step": h2d_given if upload == 2 else h2d_packed},
                         "link_h2d_gbs": link_gbs,
                         "link_what": "plain pinned-host-to-device copy of the step's bases on this machine, "
                                      "outside the timed regions"},
