@@ -271,6 +271,8 @@ typedef struct {
   uint32_t max_inflight_reads;  /* reads on the device at once (0: default) */
   uint32_t max_requests;        /* concurrently tracked requests (0: default) */
   uint64_t device_budget;       /* bytes of device memory for request buffers (0: a quarter of the free memory) */
+  uint32_t step_slots;          /* steps in flight at once, each with its own device buffers and stream
+                                 * (2-4; 0: 2) */
 } mg_server_config;
 
 int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out);

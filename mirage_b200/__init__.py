@@ -66,7 +66,8 @@ class _Tuning(C.Structure):
 
 
 class _ServerConfig(C.Structure):
-    _fields_ = [("max_inflight_reads", C.c_uint32), ("max_requests", C.c_uint32), ("device_budget", C.c_uint64)]
+    _fields_ = [("max_inflight_reads", C.c_uint32), ("max_requests", C.c_uint32), ("device_budget", C.c_uint64),
+                ("step_slots", C.c_uint32)]
 
 
 _lib = None
@@ -385,9 +386,10 @@ class Index:
 class Server:
     """Served form: continuous batching of requests against a resident index."""
 
-    def __init__(self, index: Index, max_inflight_reads: int = 0, max_requests: int = 0, device_budget: int = 0):
+    def __init__(self, index: Index, max_inflight_reads: int = 0, max_requests: int = 0, device_budget: int = 0,
+                 step_slots: int = 0):
         self.index = index
-        cfg = _ServerConfig(max_inflight_reads, max_requests, device_budget)
+        cfg = _ServerConfig(max_inflight_reads, max_requests, device_budget, step_slots)
         h = C.c_void_p()
         _check(lib().mg_server_create(index.h, C.byref(cfg), C.byref(h)), "mg_server_create")
         self.h = h

@@ -83,7 +83,10 @@ struct mg_server {
   uint64_t next_ticket = 1;
   std::deque<mg::Request*> queue;                          // requests with unscheduled reads
   std::map<uint64_t, std::unique_ptr<mg::Request>> live;   // every tracked request
-  mg::Slot slot[2];
+  static constexpr int kMaxSlots = 4;
+  mg::Slot slot[kMaxSlots];
+  int n_slots = 2;                  // step slots in use (mg_server_config.step_slots)
+  std::deque<int> in_flight;        // busy slots in launch order
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
@@ -338,30 +341,25 @@ static void drain_step(mg_server* sv, Slot& s) {
 
 static void server_loop(mg_server* sv) {
   cudaSetDevice(sv->ix->device);
-  int oldest = 0;
   std::unique_lock<std::mutex> lk(sv->mu);
   for (;;) {
-    sv->cv_work.wait(lk, [&] { return sv->stop || !sv->queue.empty() || sv->slot[0].busy || sv->slot[1].busy; });
-    if (sv->stop && !sv->slot[0].busy && !sv->slot[1].busy) break;
+    sv->cv_work.wait(lk, [&] { return sv->stop || !sv->queue.empty() || !sv->in_flight.empty(); });
+    if (sv->stop && sv->in_flight.empty()) break;
     // launch into every free slot while there is work (asynchronous)
-    for (int i = 0; i < 2; i++) {
-      Slot& s = sv->slot[(oldest + i) % 2];
-      if (!s.busy && !sv->queue.empty()) {
+    for (int i = 0; i < sv->n_slots && !sv->queue.empty(); i++) {
+      Slot& s = sv->slot[i];
+      if (!s.busy) {
         carve_step(sv, s);
+        sv->in_flight.push_back(i);
         lk.unlock();
         launch_step(sv, s);
         lk.lock();
       }
     }
-    // drain the oldest busy slot
-    Slot* d = nullptr;
-    for (int i = 0; i < 2; i++)
-      if (sv->slot[(oldest + i) % 2].busy) {
-        d = &sv->slot[(oldest + i) % 2];
-        oldest = (oldest + i + 1) % 2;
-        break;
-      }
-    if (!d) continue;
+    // drain the oldest launched step
+    if (sv->in_flight.empty()) continue;
+    Slot* d = &sv->slot[sv->in_flight.front()];
+    sv->in_flight.pop_front();
     lk.unlock();
     drain_step(sv, *d);
     lk.lock();
@@ -380,7 +378,7 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
   if (cudaSetDevice(ix->device) != cudaSuccess) return set_error(MG_ERR_CUDA, "cudaSetDevice");
   mg_server* sv = new mg_server();
   sv->ix = ix;
-  mg_server_config c = cfg ? *cfg : mg_server_config{0, 0, 0};
+  mg_server_config c = cfg ? *cfg : mg_server_config{0, 0, 0, 0};
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   // device memory for the two step slots: ~0.6 KB per read of a step
@@ -393,13 +391,15 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
   sv->step_reads = reads;
   sv->step_bases = reads * 320;
   sv->max_requests = c.max_requests ? c.max_requests : 4096;
-  // pinned ring for queued requests: 4 steps' worth of reads, at least 64 MB
-  sv->ring.cap = std::max<uint64_t>(64ull << 20, 4 * (sv->step_bases + (sv->step_reads + 1) * 8));
+  sv->n_slots = c.step_slots ? (int)std::min<uint32_t>(std::max<uint32_t>(c.step_slots, 2), mg_server::kMaxSlots) : 2;
+  // pinned ring for queued requests: (slots + 2) steps' worth of reads, at least 64 MB
+  sv->ring.cap = std::max<uint64_t>(64ull << 20, (uint64_t)(sv->n_slots + 2) * (sv->step_bases + (sv->step_reads + 1) * 8));
   if (cudaMallocHost((void**)&sv->ring.base, sv->ring.cap) != cudaSuccess) {
     delete sv;
     return set_error(MG_ERR_OOM, "pinned request ring");
   }
-  for (auto& s : sv->slot) {
+  for (int i = 0; i < sv->n_slots; i++) {
+    Slot& s = sv->slot[i];
     if (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess ||
         slot_alloc(s, sv->step_reads, sv->step_bases, 16 * sv->step_reads + 1024) != MG_OK) {
       for (auto& t : sv->slot) slot_free(t);
