@@ -46,6 +46,7 @@ enum : int {
   kErrOutput = 4,     // candidate buffer too small
   kErrLogRange = 8,   // relative-score log outside the patched domain
   kErrArena = 16,     // staging arena too small for the reads with more than kSlots candidates
+  kErrInternal = 32,  // a bounded device loop reached its bound (an invariant failed)
 };
 
 struct BatchDev {

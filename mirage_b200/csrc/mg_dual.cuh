@@ -146,7 +146,8 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
     if (i < T) {
       const uint32_t ref = e_ref[i];
       uint32_t x = (ref * 2654435761u) >> (Cap == 64 ? 26 : Cap == 128 ? 25 : 24);  // Cap entries
-      for (;;) {
+      // at most T <= Cap distinct references: a free or matching entry is found within Cap probes
+      for (int n = 0; n < Cap; n++) {
         const uint32_t old = atomicCAS(&tkey[x], EMPTY, ref);
         if (old == EMPTY || old == ref) break;
         x = (x + 1) & (Cap - 1);

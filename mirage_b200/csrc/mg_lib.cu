@@ -1270,6 +1270,7 @@ int error_status(int err) {
   if (err & kErrOutput) return set_error(MG_ERR_OOM, "candidate output buffer too small");
   if (err & kErrLogRange) return set_error(MG_ERR_LIMIT, "relative-score logarithm outside its exact domain");
   if (err & kErrArena) return set_error(MG_ERR_OOM, "staging arena too small");
+  if (err & kErrInternal) return set_error(MG_ERR_CUDA, "a device loop reached its bound (internal error)");
   return MG_OK;
 }
 

@@ -51,22 +51,29 @@ static_assert(kLgK * 12 <= 2 * kLgE * 4 && kLgQ / 32 + 1 <= kLgE, "aliased regio
 
 __device__ __forceinline__ uint32_t lg_mix(uint32_t x) { return (x * 2654435761u) ^ (x >> 15); }
 
-__device__ __forceinline__ bool lg_contains(const uint32_t* set, uint32_t mask, uint32_t key) {
-  for (uint32_t s = lg_mix(key) & mask;; s = (s + 1) & mask) {
+// The probes visit each slot at most once: every caller keeps its table at most half full, so an
+// empty slot ends them first; reaching the bound sets kErrInternal in *err.
+__device__ __forceinline__ bool lg_contains(const uint32_t* set, uint32_t mask, uint32_t key, int* err) {
+  uint32_t s = lg_mix(key) & mask;
+  for (uint32_t n = 0; n <= mask; n++, s = (s + 1) & mask) {
     const uint32_t v = set[s];
     if (v == key) return true;
     if (v == kLgEmpty) return false;
   }
+  *err |= kErrInternal;
+  return false;
 }
 
-// Inserts key; true when this call inserted it (false: it was there already). Every caller keeps
-// its table at most half full, so an empty slot is always found.
-__device__ __forceinline__ bool lg_insert(uint32_t* set, uint32_t mask, uint32_t key) {
-  for (uint32_t s = lg_mix(key) & mask;; s = (s + 1) & mask) {
+// Inserts key; true when this call inserted it (false: it was there already).
+__device__ __forceinline__ bool lg_insert(uint32_t* set, uint32_t mask, uint32_t key, int* err) {
+  uint32_t s = lg_mix(key) & mask;
+  for (uint32_t n = 0; n <= mask; n++, s = (s + 1) & mask) {
     const uint32_t old = atomicCAS(&set[s], kLgEmpty, key);
     if (old == kLgEmpty) return true;
     if (old == key) return false;
   }
+  *err |= kErrInternal;
+  return false;
 }
 
 // One strand of a read (raw bytes, L <= kLgQ) on the whole block. Same contract as
@@ -165,16 +172,16 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
   }
   __syncthreads();
   for (uint32_t i = tid; i < ne; i += G)
-    if (lg_insert(S.hs, mask, (S.p_ref[i] << 11) | (S.p_fj[i] & 0x7FFu))) S.p_fj[i] |= 0x80000000u;
+    if (lg_insert(S.hs, mask, (S.p_ref[i] << 11) | (S.p_fj[i] & 0x7FFu), err)) S.p_fj[i] |= 0x80000000u;
   __syncthreads();
   // occurrence runs from their first found index: the longest is hs
   auto run_from = [&](uint32_t i) -> uint32_t {  // 0 unless posting i starts a run
     const uint32_t fj = S.p_fj[i];
     if (!(fj >> 31)) return 0;
     const uint32_t key = (S.p_ref[i] << 11) | (fj & 0x7FFu);
-    if ((fj & 0x7FFu) && lg_contains(S.hs, mask, key - 1)) return 0;
+    if ((fj & 0x7FFu) && lg_contains(S.hs, mask, key - 1, err)) return 0;
     uint32_t len = 1;
-    while ((fj & 0x7FFu) + len < nf && lg_contains(S.hs, mask, key + len)) len++;
+    while ((fj & 0x7FFu) + len < nf && lg_contains(S.hs, mask, key + len, err)) len++;
     return len;
   };
   uint32_t mx = 0;
@@ -189,8 +196,8 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
   // table never fills, and a refused one leaves n_rt above kLgRT / 2, which sends the strand to the
   // block tier
   for (uint32_t i = tid; i < ne; i += G)
-    if (run_from(i) >= keep_min && !lg_contains(S.rt, kLgRT - 1, S.p_ref[i]))
-      if (atomicAdd(&S.n_rt, 1u) < (uint32_t)kLgRT / 2) lg_insert(S.rt, kLgRT - 1, S.p_ref[i]);
+    if (run_from(i) >= keep_min && !lg_contains(S.rt, kLgRT - 1, S.p_ref[i], err))
+      if (atomicAdd(&S.n_rt, 1u) < (uint32_t)kLgRT / 2) lg_insert(S.rt, kLgRT - 1, S.p_ref[i], err);
   __syncthreads();
   if (S.n_rt > (uint32_t)kLgRT / 2) return kStrandOverflow;
   // 3. the kept references' postings, as (refID << 32 | position, query position) sort keys
@@ -198,7 +205,7 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
   uint32_t* kB = S.hs + 2 * kLgK;
   for (uint32_t i = tid; i < ne; i += G) {
     const uint32_t ref = S.p_ref[i];
-    if (lg_contains(S.rt, kLgRT - 1, ref)) {
+    if (lg_contains(S.rt, kLgRT - 1, ref, err)) {
       const uint32_t t = atomicAdd(&S.n_kept, 1u);
       if (t < (uint32_t)kLgK) {
         kA[t] = ((uint64_t)ref << 32) | S.p_pos[i];
@@ -342,8 +349,8 @@ __device__ bool process_read_long(const DevIndex& ix, const BatchDev& b, uint32_
   uint32_t n[2] = {0, 0};
   float h[2] = {-1.0f, -1.0f};
   int st = long_strand(ix, raw, L, 0, S, &err, &n[0], &h[0]);
-  if (st == kStrandOverflow) return false;
-  if (st != kStrandBad) st = long_strand(ix, raw, L, 1, S, &err, &n[1], &h[1]);
+  if (st != kStrandBad && st != kStrandOverflow) st = long_strand(ix, raw, L, 1, S, &err, &n[1], &h[1]);
+  if (err & kErrInternal) atomicOr(errw, kErrInternal);  // any thread's: the probes record it per thread
   if (st == kStrandOverflow) return false;
   if (threadIdx.x == 0)
     write_read_result_s(b, r, st == kStrandBad, n[0], n[1], h[0], h[1], S.cb[0], S.cb[1], stage, arena, arena_cap,
