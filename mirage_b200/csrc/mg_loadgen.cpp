@@ -61,7 +61,7 @@ struct Client {
   std::vector<std::unique_ptr<Buf>> pool;
   uint64_t reads_done = 0, requests = 0;
   int error = 0;
-  explicit Client(uint64_t seed, uint32_t max_req) : rng(seed), o(max_req + 1) {}
+  explicit Client(uint64_t seed, uint32_t max_req) : rng(seed), o(max_req + 1), buf_reads(max_req) {}
 
   // a request: (first read, size); its offsets rebased into o
   mg_batch draw(const Pool& p, uint32_t* size_out) {
@@ -75,20 +75,28 @@ struct Client {
     *size_out = (uint32_t)size;
     return mg_batch{size, o.data(), p.bases + b0};
   }
-  Buf* acquire(uint64_t n, uint64_t n_cands) {
-    std::lock_guard<std::mutex> lk(pool_mu);
-    for (size_t i = 0; i < pool.size(); i++)
-      if (pool[i]->reads.size() >= n && pool[i]->cands.size() >= n_cands) {
-        Buf* b = pool[i].release();
-        pool.erase(pool.begin() + (long)i);
+  // Buffers of one size, for the largest request (max_req reads, 4 candidates per read, more
+  // on demand), made and touched before the measurement (warm), reused last in, first out.
+  uint64_t buf_reads = 0;
+  Buf* make_buf() {
+    Buf* b = new Buf();
+    b->reads.assign(buf_reads, mg_read_result{});
+    b->cands.assign(4 * buf_reads + 64, mg_candidate{});
+    return b;
+  }
+  void warm(int n) {
+    for (int i = 0; i < n; i++) pool.emplace_back(make_buf());
+  }
+  Buf* acquire() {
+    {
+      std::lock_guard<std::mutex> lk(pool_mu);
+      if (!pool.empty()) {
+        Buf* b = pool.back().release();
+        pool.pop_back();
         return b;
       }
-    Buf* b = new Buf();
-    uint64_t cap = 1;
-    while (cap < n) cap <<= 1;  // powers of two, so buffers are reused across sizes
-    b->reads.assign(cap, mg_read_result{});
-    b->cands.assign(std::max<uint64_t>(16 * cap + 64, n_cands), mg_candidate{});
-    return b;
+    }
+    return make_buf();  // more requests outstanding than were warmed
   }
   void release(Buf* b) {
     std::lock_guard<std::mutex> lk(pool_mu);
@@ -132,7 +140,7 @@ void closed_loop(mg_server* sv, const Pool& p, Client& c, Clock::time_point end,
     uint32_t size;
     const mg_batch b = c.draw(p, &size);
     uint64_t t;
-    Buf* buf = c.acquire(size, 16ull * size + 64);
+    Buf* buf = c.acquire();
     const auto t0 = Clock::now();
     if (int rc = c.submit(sv, b, buf, &t)) {
       c.release(buf);
@@ -194,7 +202,7 @@ void open_loop(mg_server* sv, const Pool& p, Client& c, Clock::time_point start,
     uint32_t size;
     const mg_batch b = c.draw(p, &size);
     uint64_t t;
-    Buf* buf = c.acquire(size, 16ull * size + 64);
+    Buf* buf = c.acquire();
     if (int rc = c.submit(sv, b, buf, &t)) {
       c.release(buf);
       c.error = rc;
@@ -223,7 +231,10 @@ extern "C" int mg_loadgen_run(mg_server* sv, const uint64_t* offs, const uint8_t
     return MG_ERR_INVAL;
   Pool p{offs, bases, n_reads, (uint32_t)std::min<uint64_t>(max_req, n_reads)};
   std::vector<std::unique_ptr<Client>> cl;
-  for (int i = 0; i < clients; i++) cl.emplace_back(new Client(seed + 7919ull * (uint64_t)i, p.max_req));
+  for (int i = 0; i < clients; i++) {
+    cl.emplace_back(new Client(seed + 7919ull * (uint64_t)i, p.max_req));
+    cl.back()->warm(rate_reads_s > 0 ? 16 : std::max(1, depth) + 1);  // before the clock starts
+  }
   const double mean_size = p.max_req > 1 ? (double)(p.max_req - 1) / std::log((double)p.max_req) : 1.0;
   const auto t0 = Clock::now();
   std::vector<std::thread> th;
