@@ -78,6 +78,7 @@ struct mg_server {
   uint64_t dev_budget = 0, dev_booked = 0;  // admission: device bytes of the admitted requests
   uint64_t dev_cap = 0;                     // the budget set at creation (the budget's ceiling)
   uint64_t dev_reserve = 0;                 // free device memory kept for the step buffers' growth
+  std::chrono::steady_clock::time_point budget_read{};  // last read of the device's free memory
   uint32_t max_requests = 0;
   mg::Ring ring;
   uint64_t next_ticket = 1;
@@ -126,6 +127,8 @@ static void slot_free(Slot& s) {
   if (s.h_cands) cudaFreeHost(s.h_cands);
   s.ws.release();
 }
+
+constexpr std::chrono::milliseconds kBudgetRefresh{50};
 
 // Take a step's worth of request segments from the queue (server lock held).
 static void carve_step(mg_server* sv, Slot& s) {
@@ -313,9 +316,15 @@ static void drain_step(mg_server* sv, Slot& s) {
     deliver_range(cut[0], cut[1]);
     for (std::thread& h : helpers) h.join();
   }
-  // the device budget follows the device's free memory (read outside the lock)
+  // the device budget follows the device's free memory, read outside the lock at most every
+  // kBudgetRefresh (the query is a driver call, too slow for every step of the server thread)
   size_t free_b = 0, total_b = 0;
-  const bool have_free = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
+  bool have_free = false;
+  const auto now = std::chrono::steady_clock::now();
+  if (now - sv->budget_read >= kBudgetRefresh) {
+    have_free = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
+    sv->budget_read = now;
+  }
   std::lock_guard<std::mutex> lk(sv->mu);
   if (have_free) {
     const uint64_t room = free_b > sv->dev_reserve ? free_b - sv->dev_reserve : 0;
