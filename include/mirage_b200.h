@@ -285,6 +285,27 @@ int mg_server_submit(mg_server* s, const mg_batch* batch, uint64_t* ticket);
  * there; out->n_cands of the submitted struct receives the count). When the candidates exceed
  * out->cand_cap the request completes with MG_ERR_OOM and n_cands holds the number needed. */
 int mg_server_submit_into(mg_server* s, const mg_batch* batch, mg_result* out, uint64_t* ticket);
+/* Page-locks the host range [ptr, ptr + len) for the server (cudaHostRegister). A request
+ * submitted afterwards whose bases lie inside a registered range is copied to the device
+ * straight from the caller's memory rather than through the request ring (its offsets are
+ * still copied), so the caller keeps those bases unchanged until the request is complete.
+ * Memory that is page-locked already (cudaMallocHost, cudaHostRegister) is refused with
+ * MG_ERR_INVAL: the server reads directly only from ranges that it registered itself. Ranges
+ * stay registered, and must stay allocated, until mg_server_destroy. */
+int mg_server_register_host(mg_server* s, const void* ptr, uint64_t len);
+/* Where the server's time went since mg_server_create (seconds; the server thread's phases sum
+ * to its lifetime). */
+typedef struct {
+  uint64_t steps, reads, requests;
+  uint64_t ring_bytes;    /* bases that submit copied into the request ring */
+  uint64_t direct_bytes;  /* bases copied to the device from registered caller memory */
+  double submit_copy_s;   /* submit: copying requests into the ring, summed over the callers */
+  double launch_s;        /* server thread: forming steps, host-to-device copies, launches */
+  double device_s;        /* server thread: waiting for steps and their result copies */
+  double deliver_s;       /* server thread: handing results to requests */
+  double idle_s;          /* server thread: waiting for requests */
+} mg_server_stats;
+int mg_server_get_stats(mg_server* s, mg_server_stats* out);
 /* Non-blocking: returns 1 and fills out when the request is complete, 0 when not yet. */
 int mg_server_poll(mg_server* s, uint64_t ticket, mg_result* out);
 /* Blocking variant of mg_server_poll with a timeout in milliseconds (MG_ERR_TIMEOUT). */

@@ -27,7 +27,8 @@ EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_insp
            "mg_set_timing", "mg_set_probe_slots", "mg_set_tuning", "mg_get_tuning", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
            "mg_build_image", "mg_build_image_device", "mg_parse_fasta_device", "mg_seqs_free", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
-           "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_submit_into", "mg_server_poll",
+           "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_submit_into", "mg_server_register_host",
+           "mg_server_get_stats", "mg_server_poll",
            "mg_server_wait", "mg_server_destroy", "mg_strerror", "mg_last_error", "mg_logs_open", "mg_logs_write",
            "mg_logs_close", "mg_make_results_dir", "mg_index_reference"]
 
@@ -70,6 +71,12 @@ class _ServerConfig(C.Structure):
                 ("step_slots", C.c_uint32)]
 
 
+class _ServerStats(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("reads", C.c_uint64), ("requests", C.c_uint64), ("ring_bytes", C.c_uint64),
+                ("direct_bytes", C.c_uint64), ("submit_copy_s", C.c_double), ("launch_s", C.c_double),
+                ("device_s", C.c_double), ("deliver_s", C.c_double), ("idle_s", C.c_double)]
+
+
 _lib = None
 
 
@@ -104,6 +111,8 @@ def lib() -> C.CDLL:
         L.mg_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
         L.mg_server_submit.argtypes = [vp, C.POINTER(_Batch), C.POINTER(u64)]
         L.mg_server_submit_into.argtypes = [vp, C.POINTER(_Batch), C.POINTER(_Result), C.POINTER(u64)]
+        L.mg_server_register_host.argtypes = [vp, vp, u64]
+        L.mg_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
         L.mg_server_poll.argtypes = [vp, u64, C.POINTER(_Result)]
         L.mg_server_wait.argtypes = [vp, u64, C.POINTER(_Result), C.c_uint32]
         L.mg_server_destroy.argtypes = [vp]
@@ -395,6 +404,23 @@ class Server:
         self.h = h
         self._pending: dict[int, int] = {}
         self._into: dict[int, tuple] = {}  # ticket -> (reads, cands, result struct) of submit_into
+        self._registered: list = []  # arrays page-locked by register_host (kept alive with the server)
+
+    def register_host(self, array) -> None:
+        """Page-lock a host array for the server (mg_server_register_host): requests whose bases
+        lie in it are copied to the device from it, without the copy into the request ring. The
+        array must stay unchanged while such requests are outstanding."""
+        a = np.ascontiguousarray(array)
+        if a is not array and isinstance(array, np.ndarray):
+            raise ValueError("register_host needs a contiguous array")
+        _check(lib().mg_server_register_host(self.h, a.ctypes.data, a.nbytes), "mg_server_register_host")
+        self._registered.append(a)
+
+    def stats(self) -> dict:
+        """Counters and the server thread's time per phase since creation (mg_server_get_stats)."""
+        st = _ServerStats()
+        _check(lib().mg_server_get_stats(self.h, C.byref(st)), "mg_server_get_stats")
+        return {f: getattr(st, f) for f, _ in _ServerStats._fields_}
 
     def submit(self, bases, offsets) -> int | None:
         """Submit a request; returns its ticket, or None when it cannot be admitted now."""

@@ -14,7 +14,9 @@
 // take in a step (bases, offsets, results and a candidate allowance) against a budget, which
 // follows the device's free memory as steps complete (another user's allocations shrink it).
 // A request submitted with caller buffers (mg_server_submit_into) has its results written into
-// them by the server's delivery threads, with no copy at completion.
+// them by the server's delivery threads, with no copy at completion. A request whose bases lie in
+// host memory the server has page-locked for the caller (mg_server_register_host) is copied to
+// the device from there, so submit copies only its offsets.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,8 +39,8 @@ namespace mg {
 struct Request {
   uint64_t ticket = 0;
   uint64_t n = 0;
-  uint64_t* offs = nullptr;   // in the pinned ring: n + 1 offsets
-  uint8_t* bases = nullptr;   // in the pinned ring
+  uint64_t* offs = nullptr;     // in the pinned ring: n + 1 offsets
+  const uint8_t* bases = nullptr;  // in the pinned ring, or in a range registered by the caller
   uint64_t ring_at = 0;
   uint64_t next = 0;  // next read to schedule
   uint64_t done = 0;  // reads with results
@@ -88,6 +90,14 @@ struct mg_server {
   mg::Slot slot[kMaxSlots];
   int n_slots = 2;                  // step slots in use (mg_server_config.step_slots)
   std::deque<int> in_flight;        // busy slots in launch order
+  struct HostRange {
+    uintptr_t p;
+    uint64_t len;
+  };
+  std::vector<HostRange> host_ranges;  // page-locked by mg_server_register_host (under mu)
+  // mg_server_get_stats
+  std::atomic<uint64_t> n_steps{0}, n_reads{0}, n_requests{0}, ring_bytes{0}, direct_bytes{0};
+  std::atomic<uint64_t> ns_submit{0}, ns_launch{0}, ns_device{0}, ns_deliver{0}, ns_idle{0};
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
@@ -129,6 +139,11 @@ static void slot_free(Slot& s) {
 }
 
 constexpr std::chrono::milliseconds kBudgetRefresh{50};
+using Clock = std::chrono::steady_clock;
+
+static uint64_t ns_since(Clock::time_point t0) {
+  return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - t0).count();
+}
 
 // Take a step's worth of request segments from the queue (server lock held).
 static void carve_step(mg_server* sv, Slot& s) {
@@ -198,6 +213,7 @@ static void launch_step(mg_server* sv, Slot& s) {
 // Wait for a launched step and hand its results to the requests (server lock not held while
 // waiting on the device).
 static void drain_step(mg_server* sv, Slot& s) {
+  const auto t_wait = Clock::now();
   int rc = s.launch_rc;
   Counters c;
   if (rc != MG_OK) cudaStreamSynchronize(s.st);  // copies from the ring may still be in flight
@@ -233,6 +249,8 @@ static void drain_step(mg_server* sv, Slot& s) {
         cudaStreamSynchronize(s.st) != cudaSuccess)
       rc = set_error(MG_ERR_CUDA, "step results");
   }
+  const auto t_deliver = Clock::now();
+  sv->ns_device += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(t_deliver - t_wait).count();
   // results to the requests without the lock: until a request completes, only the server writes
   // its result vectors and error code, and a step holds at most one segment of each request, so
   // the segments can be delivered in parallel
@@ -330,11 +348,14 @@ static void drain_step(mg_server* sv, Slot& s) {
     const uint64_t room = free_b > sv->dev_reserve ? free_b - sv->dev_reserve : 0;
     sv->dev_budget = std::min(sv->dev_cap, room + sv->dev_booked);
   }
+  sv->n_steps++;
+  sv->n_reads += s.n;
   for (const Part& p : s.parts) {
     Request* r = p.req;
     r->done += p.count;
     if (r->done == r->n) {
       r->complete = true;
+      sv->n_requests++;
       if (!r->released) {
         sv->ring.release(r->ring_at);
         r->released = true;
@@ -345,6 +366,7 @@ static void drain_step(mg_server* sv, Slot& s) {
   }
   s.parts.clear();
   s.busy = false;
+  sv->ns_deliver += ns_since(t_deliver);
   sv->cv_done.notify_all();
 }
 
@@ -352,7 +374,9 @@ static void server_loop(mg_server* sv) {
   cudaSetDevice(sv->ix->device);
   std::unique_lock<std::mutex> lk(sv->mu);
   for (;;) {
+    const auto t_idle = Clock::now();
     sv->cv_work.wait(lk, [&] { return sv->stop || !sv->queue.empty() || !sv->in_flight.empty(); });
+    sv->ns_idle += ns_since(t_idle);
     if (sv->stop && sv->in_flight.empty()) break;
     // launch into every free slot while there is work (asynchronous)
     for (int i = 0; i < sv->n_slots && !sv->queue.empty(); i++) {
@@ -361,7 +385,9 @@ static void server_loop(mg_server* sv) {
         carve_step(sv, s);
         sv->in_flight.push_back(i);
         lk.unlock();
+        const auto t_launch = Clock::now();
         launch_step(sv, s);
+        sv->ns_launch += ns_since(t_launch);
         lk.lock();
       }
     }
@@ -439,13 +465,20 @@ static int submit(mg_server* sv, const mg_batch* b, mg_result* dst, uint64_t* ti
   for (uint64_t i = 0; i < n; i++)
     if (b->offsets[i + 1] < b->offsets[i] || b->offsets[i + 1] - b->offsets[i] > 65535)
       return set_error(MG_ERR_LIMIT, "read longer than 65535 bases");
-  const uint64_t len = nb + (n + 1) * 8 + 16;
   std::unique_ptr<Request> r(new Request());
   r->n = n;
   r->dst = dst;
   const uint64_t dev = request_device_bytes(n, nb);
+  bool direct = false;  // bases read in place, from a range registered with the server
   {
     std::lock_guard<std::mutex> lk(sv->mu);
+    const uintptr_t b0 = (uintptr_t)b->bases;
+    for (const auto& h : sv->host_ranges)
+      if (nb && b0 >= h.p && b0 - h.p <= h.len && nb <= h.len - (b0 - h.p)) {
+        direct = true;
+        break;
+      }
+    const uint64_t len = (direct ? 0 : nb) + (n + 1) * 8 + 16;
     if (len > sv->ring.cap) return set_error(MG_ERR_LIMIT, "request larger than the server's request memory");
     if (dev > sv->dev_cap) return set_error(MG_ERR_LIMIT, "request larger than the server's device budget");
     if (sv->dev_booked + dev > sv->dev_budget) return set_error(MG_ERR_BUSY, "not enough free device memory now");
@@ -454,10 +487,17 @@ static int submit(mg_server* sv, const mg_batch* b, mg_result* dst, uint64_t* ti
     sv->dev_booked += dev;
     r->dev_bytes = dev;
     r->offs = (uint64_t*)(sv->ring.base + r->ring_at);
-    r->bases = sv->ring.base + r->ring_at + (n + 1) * 8;
+    r->bases = direct ? b->bases : sv->ring.base + r->ring_at + (n + 1) * 8;
   }
+  const auto t_copy = Clock::now();
   std::memcpy(r->offs, b->offsets, (n + 1) * 8);
-  std::memcpy(r->bases, b->bases, nb);
+  if (direct) {
+    sv->direct_bytes += nb;
+  } else {
+    std::memcpy(sv->ring.base + r->ring_at + (n + 1) * 8, b->bases, nb);
+    sv->ring_bytes += nb;
+  }
+  sv->ns_submit += ns_since(t_copy);
   if (!dst) {
     try {
       r->reads.resize(n);
@@ -542,6 +582,35 @@ int mg_server_wait(mg_server* sv, uint64_t ticket, mg_result* out, uint32_t time
   return take_result(sv, sv->live.find(ticket), out, lk);
 }
 
+int mg_server_register_host(mg_server* sv, const void* ptr, uint64_t len) {
+  if (!sv || !ptr || !len) return set_error(MG_ERR_INVAL, "null argument");
+  if (cudaSetDevice(sv->ix->device) != cudaSuccess) return set_error(MG_ERR_CUDA, "cudaSetDevice");
+  const cudaError_t e = cudaHostRegister(const_cast<void*>(ptr), len, cudaHostRegisterDefault);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // not sticky: clear it
+    if (e == cudaErrorHostMemoryAlreadyRegistered) return set_error(MG_ERR_INVAL, "range is page-locked already");
+    return set_error(MG_ERR_CUDA, cudaGetErrorString(e));
+  }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->host_ranges.push_back(mg_server::HostRange{(uintptr_t)ptr, len});
+  return MG_OK;
+}
+
+int mg_server_get_stats(mg_server* sv, mg_server_stats* out) {
+  if (!sv || !out) return set_error(MG_ERR_INVAL, "null argument");
+  out->steps = sv->n_steps;
+  out->reads = sv->n_reads;
+  out->requests = sv->n_requests;
+  out->ring_bytes = sv->ring_bytes;
+  out->direct_bytes = sv->direct_bytes;
+  out->submit_copy_s = sv->ns_submit * 1e-9;
+  out->launch_s = sv->ns_launch * 1e-9;
+  out->device_s = sv->ns_device * 1e-9;
+  out->deliver_s = sv->ns_deliver * 1e-9;
+  out->idle_s = sv->ns_idle * 1e-9;
+  return MG_OK;
+}
+
 void mg_server_destroy(mg_server* sv) {
   if (!sv) return;
   {
@@ -554,6 +623,7 @@ void mg_server_destroy(mg_server* sv) {
   cudaSetDevice(sv->ix->device);
   for (auto& s : sv->slot) slot_free(s);
   if (sv->ring.base) cudaFreeHost(sv->ring.base);
+  for (const auto& h : sv->host_ranges) cudaHostUnregister((void*)h.p);
   sv->ix->n_servers--;
   delete sv;
 }

@@ -166,3 +166,52 @@ def test_admission_by_device_budget(golden):
     assert t3 is not None
     same(sv.wait(t3), ix.classify(d, o))
     sv.close()
+
+
+def test_bases_read_in_place_from_registered_memory(golden):
+    """mg_server_register_host: requests whose bases lie in a range the server page-locked are
+    copied to the device from there (only their offsets go through the request ring); their
+    results equal the copying path's. The counters of mg_server_get_stats add up: bytes in place
+    and through the ring, reads, requests. Memory already page-locked, or registered twice, is
+    refused with MG_ERR_INVAL."""
+    import torch
+
+    g = golden("uneven_small")
+    ix = M.Index(g.image)
+    pool = np.array(g.reads.data, dtype=np.uint8, copy=True)  # pageable, owned here
+    rng = np.random.default_rng(11)
+    cuts = np.unique(np.concatenate([[0, len(g.reads)], rng.integers(1, len(g.reads), size=24)]))
+    offs = g.reads.offs
+    parts = []
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        o0, o1 = int(offs[a]), int(offs[b])
+        parts.append((pool[o0:o1], (offs[a : b + 1] - offs[a]).astype(np.uint64)))
+    alone = [ix.classify(d, o) for d, o in parts]
+    sv = M.Server(ix, max_inflight_reads=1024)
+    sv.register_host(pool)
+    with pytest.raises(M.MirageError) as e:
+        sv.register_host(pool)
+    assert e.value.code == -8
+    pinned = torch.empty(1 << 16, dtype=torch.uint8, pin_memory=True)
+    with pytest.raises(M.MirageError) as e:
+        sv.register_host(pinned.numpy())
+    assert e.value.code == -8
+    # even parts in place, odd parts copied (a copy of the slice lies outside the registered range)
+    tickets, direct, ring = [], 0, 0
+    for i, (d, o) in enumerate(parts):
+        src = d if i % 2 == 0 else d.copy()
+        t = sv.submit_into(src, o) if i % 3 else sv.submit(src, o)
+        assert t is not None
+        tickets.append(t)
+        if i % 2 == 0:
+            direct += len(d)
+        else:
+            ring += len(d)
+    for a, t in zip(alone, tickets):
+        same(a, sv.wait(t))
+    st = sv.stats()
+    assert st["direct_bytes"] == direct and st["ring_bytes"] == ring
+    assert st["reads"] == len(g.reads) and st["requests"] == len(parts) and st["steps"] >= 1
+    for k in ("submit_copy_s", "launch_s", "device_s", "deliver_s", "idle_s"):
+        assert st[k] >= 0.0
+    sv.close()
