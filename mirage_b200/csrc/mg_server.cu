@@ -5,19 +5,25 @@
 // it can never fit). A server thread forms "steps" from the queued reads in arrival order (a
 // large request spans several steps, one step carries reads of many requests) and runs the
 // fused pipeline on them; each request segment of a step is one host->device copy straight from
-// the ring. Two step slots, each with its own device workspace and stream, let the next step's
-// copies and kernels run while the previous step's results are drained. A request arriving
-// while steps are on the device joins the next step formed. Each read is classified on its
-// own, so a request's results are the same alone and in any mix.
+// the ring. Step slots (2 to 4), each with its own device workspace and stream, let the next
+// step's copies and kernels run while earlier steps finish. A request arriving while steps are on
+// the device joins the next step formed. Each read is classified on its own, so a request's
+// results are the same alone and in any mix.
+//
+// Threads: the server thread carves, launches and waits for steps; a delivery thread hands each
+// finished step's results to its requests, in launch order, and frees its slot. Each has a few
+// worker threads for the per-read host work (rebasing offsets into the step; copying results out),
+// split in pieces of at most 32,768 reads.
 //
 // Admission also holds device memory: each admitted request books the device bytes its reads
 // take in a step (bases, offsets, results and a candidate allowance) against a budget, which
 // follows the device's free memory as steps complete (another user's allocations shrink it).
 // A request submitted with caller buffers (mg_server_submit_into) has its results written into
-// them by the server's delivery threads, with no copy at completion. A request whose bases lie in
+// them by the delivery thread, with no copy at completion. A request whose bases lie in
 // host memory the server has page-locked for the caller (mg_server_register_host) is copied to
 // the device from there, so submit copies only its offsets.
 #include <cuda_runtime.h>
+#include <sched.h>
 
 #include <algorithm>
 #include <atomic>
@@ -32,6 +38,7 @@
 #include <vector>
 
 #include "mg_internal.h"
+#include "mg_pack.h"
 #include "mg_ring.h"
 
 namespace mg {
@@ -59,6 +66,20 @@ struct Part {
   uint64_t first, count;  // reads [first, first+count) of req
 };
 
+// A run of at most kPieceReads consecutive reads of one part: the unit the worker threads rebase
+// offsets and deliver results in.
+struct Piece {
+  uint32_t part;
+  uint64_t at;            // first read of the piece in the step
+  uint64_t in_part;       // first read of the piece in its part
+  uint64_t count;
+  uint64_t bases_at = 0;  // launch: first base of the piece in the step
+  uint64_t base = 0;      // delivery: where the piece's first candidate goes in the request's output
+  int err = 0;            // delivery: a rejected read's error
+  bool deliver = false;   // delivery: copy this piece (the request takes it)
+};
+constexpr uint64_t kPieceReads = 32768;
+
 struct Slot {
   Workspace ws;
   cudaStream_t st = nullptr;
@@ -67,9 +88,11 @@ struct Slot {
   mg_candidate* h_cands = nullptr;
   uint64_t cap_reads = 0, cap_cands = 0;
   std::vector<Part> parts;
+  std::vector<Piece> pieces;
   uint64_t n = 0;
-  bool busy = false;
+  bool busy = false;      // from carving until its results are delivered
   int launch_rc = 0;
+  int drain_rc = 0;       // the step's status after the device part of draining
 };
 
 }  // namespace mg
@@ -89,7 +112,12 @@ struct mg_server {
   static constexpr int kMaxSlots = 4;
   mg::Slot slot[kMaxSlots];
   int n_slots = 2;                  // step slots in use (mg_server_config.step_slots)
-  std::deque<int> in_flight;        // busy slots in launch order
+  std::deque<int> in_flight;        // launched slots in launch order
+  std::deque<int> to_deliver;       // drained slots in launch order, for the delivery thread
+  std::condition_variable cv_deliver;
+  bool stop_deliver = false;
+  std::thread th_deliver;
+  std::unique_ptr<mg::PackPool> pool_launch, pool_deliver;  // workers of the two threads
   struct HostRange {
     uintptr_t p;
     uint64_t len;
@@ -176,26 +204,69 @@ static void carve_step(mg_server* sv, Slot& s) {
   s.launch_rc = MG_OK;
 }
 
-// Copy a carved step's segments from the ring and launch it on the slot's stream (server lock not
-// held: the segments' requests stay queued-or-running, so their ring memory stays in place).
+// Split a step's parts into pieces of at most kPieceReads reads.
+static void make_pieces(Slot& s) {
+  s.pieces.clear();
+  uint64_t at = 0;
+  for (size_t i = 0; i < s.parts.size(); i++) {
+    for (uint64_t f = 0; f < s.parts[i].count; f += kPieceReads) {
+      Piece pc;
+      pc.part = (uint32_t)i;
+      pc.at = at + f;
+      pc.in_part = f;
+      pc.count = std::min(kPieceReads, s.parts[i].count - f);
+      s.pieces.push_back(pc);
+    }
+    at += s.parts[i].count;
+  }
+}
+
+// fn(piece) for every piece, on the pool's threads when the step is large enough to share
+template <class F>
+static void for_pieces(PackPool* pool, Slot& s, F&& fn) {
+  const size_t np = s.pieces.size();
+  if (!pool || np < 2 || s.n < 2 * kPieceReads) {
+    for (size_t i = 0; i < np; i++) fn(s.pieces[i]);
+    return;
+  }
+  const size_t T = (size_t)pool->threads();
+  pool->run([&](int t) {
+    for (size_t i = (size_t)t; i < np; i += T) fn(s.pieces[i]);
+  });
+}
+
+// Copy a carved step's segments from the ring (or the caller's registered memory) and launch it on
+// the slot's stream (server lock not held: the segments' requests stay queued-or-running, so their
+// memory stays in place). The offsets, rebased into the step, are written by the launch workers.
 static void launch_step(mg_server* sv, Slot& s) {
   if (s.n == 0) return;
+  make_pieces(s);
   uint64_t nb = 0;
-  for (const Part& p : s.parts) nb += p.req->offs[p.first + p.count] - p.req->offs[p.first];
+  for (Piece& pc : s.pieces) {
+    const Part& p = s.parts[pc.part];
+    pc.bases_at = nb;
+    const uint64_t r0 = p.first + pc.in_part;
+    nb += p.req->offs[r0 + pc.count] - p.req->offs[r0];
+  }
   if (slot_alloc(s, s.n, std::max<uint64_t>(nb, sv->step_bases), std::max<uint64_t>(s.cap_cands, 16 * s.n + 1024))) {
     s.launch_rc = MG_ERR_OOM;
     return;
   }
-  // offsets rebased into the step; bases copied segment by segment from the ring
-  uint64_t at = 0, ob = 0;
   s.h_offs[0] = 0;
+  for_pieces(sv->pool_launch.get(), s, [&](const Piece& pc) {
+    const Part& p = s.parts[pc.part];
+    const uint64_t* ro = p.req->offs + p.first + pc.in_part;
+    const uint64_t d = pc.bases_at - ro[0];  // modulo 2^64: ro[j] - ro[0] + bases_at
+    uint64_t* out = s.h_offs + pc.at + 1;
+    for (uint64_t j = 0; j < pc.count; j++) out[j] = ro[j + 1] + d;
+  });
+  // bases: one copy per part (its pieces are contiguous in the source and in the step)
   cudaError_t e = cudaSuccess;
+  uint64_t ob = 0;
   for (const Part& p : s.parts) {
     const uint64_t b0 = p.req->offs[p.first], b1 = p.req->offs[p.first + p.count];
-    for (uint64_t i = 0; i < p.count; i++) s.h_offs[at + i + 1] = ob + (p.req->offs[p.first + i + 1] - b0);
     if (e == cudaSuccess && b1 > b0)
       e = cudaMemcpyAsync(s.ws.bases.as<uint8_t>() + ob, p.req->bases + b0, b1 - b0, cudaMemcpyHostToDevice, s.st);
-    at += p.count;
     ob += b1 - b0;
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(s.ws.offs.p, s.h_offs, (s.n + 1) * 8, cudaMemcpyHostToDevice, s.st);
@@ -210,9 +281,9 @@ static void launch_step(mg_server* sv, Slot& s) {
     s.launch_rc = MG_ERR_CUDA;
 }
 
-// Wait for a launched step and hand its results to the requests (server lock not held while
-// waiting on the device).
-static void drain_step(mg_server* sv, Slot& s) {
+// Wait for a launched step and bring its results to the slot's pinned buffers (server thread;
+// lock not held). The step's status goes to s.drain_rc for the delivery thread.
+static void drain_device(mg_server* sv, Slot& s) {
   const auto t_wait = Clock::now();
   int rc = s.launch_rc;
   Counters c;
@@ -238,7 +309,7 @@ static void drain_step(mg_server* sv, Slot& s) {
     if (rc == MG_OK) rc = complete();
     reran = true;
   }
-  // a rejected read fails its own request only (below); any other error fails the step
+  // a rejected read fails its own request only (at delivery); any other error fails the step
   const int step_bits = c.err & ~(kErrBadInput | kErrLimit);
   if (rc == MG_OK && step_bits) rc = error_status(step_bits);
   if (rc == MG_OK && s.n) {
@@ -249,105 +320,92 @@ static void drain_step(mg_server* sv, Slot& s) {
         cudaStreamSynchronize(s.st) != cudaSuccess)
       rc = set_error(MG_ERR_CUDA, "step results");
   }
-  const auto t_deliver = Clock::now();
-  sv->ns_device += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(t_deliver - t_wait).count();
-  // results to the requests without the lock: until a request completes, only the server writes
-  // its result vectors and error code, and a step holds at most one segment of each request, so
-  // the segments can be delivered in parallel
-  auto deliver = [&](const Part& p, uint64_t at) {
-    Request* r = p.req;
-    if (rc != MG_OK) {
-      r->error = rc;
-      return;
+  s.drain_rc = rc;
+  // the device budget follows the device's free memory, read at most every kBudgetRefresh (the
+  // query is a driver call, too slow for every step)
+  const auto now = Clock::now();
+  if (now - sv->budget_read >= kBudgetRefresh) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      const uint64_t room = free_b > sv->dev_reserve ? free_b - sv->dev_reserve : 0;
+      sv->dev_budget = std::min(sv->dev_cap, room + sv->dev_booked);
     }
-    if (r->error) return;
-    // the segment's candidates are contiguous in the step's output (read order): one copy, into
-    // the caller's buffer when the request has one
-    const mg_read_result* src = s.h_reads + at;
-    const mg_read_result& last = src[p.count - 1];
-    const uint64_t c0 = src[0].cand_off, c1 = (uint64_t)last.cand_off + last.n_fwd + last.n_rc;
-    const uint64_t base = r->n_cands;
-    r->n_cands += c1 - c0;
+    sv->budget_read = now;
+  }
+  sv->ns_device += ns_since(t_wait);
+}
+
+// Hand a drained step's results to its requests (delivery thread; lock not held). Until a request
+// completes only this thread writes its results, count and error code, and steps are delivered in
+// launch order, so a request's segments arrive in read order. A first pass over the pieces, in
+// order, places each one in its request's output; the copies then run on the delivery workers.
+static void deliver_step(mg_server* sv, Slot& s) {
+  const auto t0 = Clock::now();
+  const int rc = s.drain_rc;
+  uint64_t c0 = 0, base = 0;  // the current part's first candidate in the step and in its request
+  for (Piece& pc : s.pieces) {
+    const Part& p = s.parts[pc.part];
+    Request* r = p.req;
+    pc.deliver = false;
+    pc.err = 0;
+    const mg_read_result* src = s.h_reads + pc.at;
+    const uint64_t pc0 = src[0].cand_off;
+    const mg_read_result& last = src[pc.count - 1];
+    const uint64_t pc1 = (uint64_t)last.cand_off + last.n_fwd + last.n_rc;
+    if (pc.in_part == 0) {  // the part's first piece: the part's candidates go after the request's
+      c0 = pc0;
+      base = r->n_cands;
+      if (rc != MG_OK) r->error = rc;
+    }
+    if (rc != MG_OK) continue;
+    if (r->error) {
+      // a request whose error came from an earlier segment still counts the candidates it needs
+      if (r->dst && r->error == MG_ERR_OOM) r->n_cands += pc1 - pc0;
+      continue;
+    }
+    r->n_cands += pc1 - pc0;
+    pc.base = base + (pc0 - c0);
     if (r->dst) {
       if (r->n_cands > r->dst->cand_cap) {
         r->error = MG_ERR_OOM;  // n_cands keeps counting what the request needs
-        return;
+        continue;
       }
-      if (c1 > c0) std::memcpy(r->dst->cands + base, s.h_cands + c0, (c1 - c0) * sizeof(mg_candidate));
     } else {
       try {
-        r->cands.insert(r->cands.end(), s.h_cands + c0, s.h_cands + c1);
+        r->cands.resize(r->n_cands);
       } catch (...) {
         r->error = MG_ERR_OOM;
-        return;
+        continue;
       }
     }
-    mg_read_result* dst = (r->dst ? r->dst->reads : r->reads.data()) + p.first;
-    for (uint64_t i = 0; i < p.count; i++) {
+    pc.deliver = true;
+  }
+  for_pieces(sv->pool_deliver.get(), s, [&](Piece& pc) {
+    if (!pc.deliver) return;
+    const Part& p = s.parts[pc.part];
+    Request* r = p.req;
+    const mg_read_result* src = s.h_reads + pc.at;
+    const uint64_t pc0 = src[0].cand_off;
+    const mg_read_result& last = src[pc.count - 1];
+    const uint64_t pc1 = (uint64_t)last.cand_off + last.n_fwd + last.n_rc;
+    mg_candidate* cd = r->dst ? r->dst->cands : r->cands.data();
+    if (pc1 > pc0) std::memcpy(cd + pc.base, s.h_cands + pc0, (pc1 - pc0) * sizeof(mg_candidate));
+    mg_read_result* dst = (r->dst ? r->dst->reads : r->reads.data()) + p.first + pc.in_part;
+    for (uint64_t i = 0; i < pc.count; i++) {
       mg_read_result rr = src[i];
       if (rr.strand == MG_READ_BAD_BYTE || rr.strand == MG_READ_TOO_LARGE) {
-        r->error = rr.strand == MG_READ_BAD_BYTE ? MG_ERR_BADINPUT : MG_ERR_LIMIT;
+        pc.err = rr.strand == MG_READ_BAD_BYTE ? MG_ERR_BADINPUT : MG_ERR_LIMIT;
         break;
       }
-      rr.cand_off = (uint32_t)(rr.cand_off - c0 + base);
+      rr.cand_off = (uint32_t)(rr.cand_off - pc0 + pc.base);
       dst[i] = rr;
     }
-  };
-  // a request whose error came from an earlier segment still counts the candidates it needs
-  auto count_only = [&](const Part& p, uint64_t at) {
-    Request* r = p.req;
-    if (rc != MG_OK || !r->dst || r->error != MG_ERR_OOM) return false;
-    const mg_read_result* src = s.h_reads + at;
-    const mg_read_result& last = src[p.count - 1];
-    r->n_cands += (uint64_t)last.cand_off + last.n_fwd + last.n_rc - src[0].cand_off;
-    return true;
-  };
-  const size_t np = s.parts.size();
-  std::vector<uint64_t> start(np + 1, 0);
-  for (size_t i = 0; i < np; i++) start[i + 1] = start[i] + s.parts[i].count;
-  auto deliver_range = [&](size_t a, size_t b) {
-    for (size_t i = a; i < b; i++)
-      if (!count_only(s.parts[i], start[i])) deliver(s.parts[i], start[i]);
-  };
-  // large steps: up to kDeliverThreads contiguous ranges of segments with about equal reads
-  constexpr int kDeliverThreads = 4;
-  constexpr uint64_t kDeliverMin = 32768;  // reads per helper thread worth its start-up
-  const int nt = (int)std::min<uint64_t>({(uint64_t)kDeliverThreads, (uint64_t)np, s.n / kDeliverMin});
-  if (nt <= 1) {
-    deliver_range(0, np);
-  } else {
-    std::vector<size_t> cut(nt + 1, np);
-    cut[0] = 0;
-    for (int t = 1, i = 0; t < nt; t++) {
-      const uint64_t want = s.n * (uint64_t)t / (uint64_t)nt;
-      while ((size_t)i < np && start[i] < want) i++;
-      cut[t] = std::max<size_t>(cut[t - 1], (size_t)i);
-    }
-    std::vector<std::thread> helpers;
-    for (int t = 1; t < nt; t++) {
-      try {
-        helpers.emplace_back(deliver_range, cut[t], cut[t + 1]);
-      } catch (...) {  // no thread: deliver this range here
-        deliver_range(cut[t], cut[t + 1]);
-      }
-    }
-    deliver_range(cut[0], cut[1]);
-    for (std::thread& h : helpers) h.join();
-  }
-  // the device budget follows the device's free memory, read outside the lock at most every
-  // kBudgetRefresh (the query is a driver call, too slow for every step of the server thread)
-  size_t free_b = 0, total_b = 0;
-  bool have_free = false;
-  const auto now = std::chrono::steady_clock::now();
-  if (now - sv->budget_read >= kBudgetRefresh) {
-    have_free = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess;
-    sv->budget_read = now;
-  }
+  });
+  for (const Piece& pc : s.pieces)
+    if (pc.err && !s.parts[pc.part].req->error) s.parts[pc.part].req->error = pc.err;
+  sv->ns_deliver += ns_since(t0);
   std::lock_guard<std::mutex> lk(sv->mu);
-  if (have_free) {
-    const uint64_t room = free_b > sv->dev_reserve ? free_b - sv->dev_reserve : 0;
-    sv->dev_budget = std::min(sv->dev_cap, room + sv->dev_booked);
-  }
   sv->n_steps++;
   sv->n_reads += s.n;
   for (const Part& p : s.parts) {
@@ -365,17 +423,28 @@ static void drain_step(mg_server* sv, Slot& s) {
     }
   }
   s.parts.clear();
+  s.pieces.clear();
   s.busy = false;
-  sv->ns_deliver += ns_since(t_deliver);
   sv->cv_done.notify_all();
+  sv->cv_work.notify_one();  // a slot is free for the server thread
 }
 
+static bool slot_free_now(const mg_server* sv) {
+  for (int i = 0; i < sv->n_slots; i++)
+    if (!sv->slot[i].busy) return true;
+  return false;
+}
+
+// Server thread: carves and launches steps into free slots and waits for each launched step in
+// turn; the delivery thread then hands its results out and frees the slot.
 static void server_loop(mg_server* sv) {
   cudaSetDevice(sv->ix->device);
   std::unique_lock<std::mutex> lk(sv->mu);
   for (;;) {
     const auto t_idle = Clock::now();
-    sv->cv_work.wait(lk, [&] { return sv->stop || !sv->queue.empty() || !sv->in_flight.empty(); });
+    sv->cv_work.wait(lk, [&] {
+      return sv->stop || (!sv->queue.empty() && slot_free_now(sv)) || !sv->in_flight.empty();
+    });
     sv->ns_idle += ns_since(t_idle);
     if (sv->stop && sv->in_flight.empty()) break;
     // launch into every free slot while there is work (asynchronous)
@@ -391,12 +460,27 @@ static void server_loop(mg_server* sv) {
         lk.lock();
       }
     }
-    // drain the oldest launched step
+    // wait for the oldest launched step, then pass it to the delivery thread
     if (sv->in_flight.empty()) continue;
-    Slot* d = &sv->slot[sv->in_flight.front()];
+    const int d = sv->in_flight.front();
     sv->in_flight.pop_front();
     lk.unlock();
-    drain_step(sv, *d);
+    drain_device(sv, sv->slot[d]);
+    lk.lock();
+    sv->to_deliver.push_back(d);
+    sv->cv_deliver.notify_one();
+  }
+}
+
+static void deliver_loop(mg_server* sv) {
+  std::unique_lock<std::mutex> lk(sv->mu);
+  for (;;) {
+    sv->cv_deliver.wait(lk, [&] { return sv->stop_deliver || !sv->to_deliver.empty(); });
+    if (sv->to_deliver.empty()) break;  // stop_deliver, nothing left
+    const int d = sv->to_deliver.front();
+    sv->to_deliver.pop_front();
+    lk.unlock();
+    deliver_step(sv, sv->slot[d]);
     lk.lock();
   }
 }
@@ -443,6 +527,18 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
       return set_error(MG_ERR_OOM, "server step buffers");
     }
   }
+  // workers for the offsets (server thread) and the results (delivery thread): a quarter of the
+  // CPUs this process may use, 1 to 4 each
+  {
+    cpu_set_t set;
+    int cpus = 0;
+    if (sched_getaffinity(0, sizeof(set), &set) == 0) cpus = CPU_COUNT(&set);
+    if (cpus <= 0) cpus = (int)std::thread::hardware_concurrency();
+    const int w = std::max(1, std::min(4, cpus / 4));
+    sv->pool_launch.reset(new PackPool(w));
+    sv->pool_deliver.reset(new PackPool(w));
+  }
+  sv->th_deliver = std::thread(deliver_loop, sv);
   sv->th = std::thread(server_loop, sv);
   ix->n_servers++;
   *out = sv;
@@ -585,6 +681,10 @@ int mg_server_wait(mg_server* sv, uint64_t ticket, mg_result* out, uint32_t time
 int mg_server_register_host(mg_server* sv, const void* ptr, uint64_t len) {
   if (!sv || !ptr || !len) return set_error(MG_ERR_INVAL, "null argument");
   if (cudaSetDevice(sv->ix->device) != cudaSuccess) return set_error(MG_ERR_CUDA, "cudaSetDevice");
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, ptr) == cudaSuccess && at.type != cudaMemoryTypeUnregistered)
+    return set_error(MG_ERR_INVAL, "range is page-locked already, or device memory");
+  cudaGetLastError();
   const cudaError_t e = cudaHostRegister(const_cast<void*>(ptr), len, cudaHostRegisterDefault);
   if (e != cudaSuccess) {
     cudaGetLastError();  // not sticky: clear it
@@ -620,6 +720,12 @@ void mg_server_destroy(mg_server* sv) {
   }
   sv->cv_work.notify_all();
   if (sv->th.joinable()) sv->th.join();
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stop_deliver = true;
+  }
+  sv->cv_deliver.notify_all();
+  if (sv->th_deliver.joinable()) sv->th_deliver.join();
   cudaSetDevice(sv->ix->device);
   for (auto& s : sv->slot) slot_free(s);
   if (sv->ring.base) cudaFreeHost(sv->ring.base);
