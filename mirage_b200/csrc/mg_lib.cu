@@ -5,6 +5,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <dlfcn.h>
+#include <sched.h>
 
 #include <algorithm>
 #include <atomic>
@@ -400,12 +401,15 @@ __global__ void __launch_bounds__(kW1Warps * 32) k_classify_warp_list(DevIndex i
 }
 
 // Long-read tier over the general warp tier's leftovers (reads beyond its limits), a block per
-// read with work stealing; its own leftovers go to the block tier.
-__global__ void __launch_bounds__(kLgThreads, 2) k_classify_long(DevIndex ix, BatchDev b, StageDev sd, const uint32_t* list,
-                                                              const unsigned* list_n, unsigned* cursor, uint32_t* next,
-                                                              unsigned* next_n) {
+// read with work stealing: the smaller size first, then the larger over what it hands on, whose
+// own leftovers go to the block tier.
+template <class SM, int MinBlocks>
+__global__ void __launch_bounds__(kLgThreads, MinBlocks) k_classify_long(DevIndex ix, BatchDev b, StageDev sd,
+                                                                      const uint32_t* list, const unsigned* list_n,
+                                                                      unsigned* cursor, uint32_t* next,
+                                                                      unsigned* next_n) {
   extern __shared__ __align__(16) uint8_t dsm[];
-  LongSmem& S = *reinterpret_cast<LongSmem*>(dsm);
+  SM& S = *reinterpret_cast<SM*>(dsm);
   __shared__ uint32_t s_item;
   const uint32_t n = *list_n;
   for (;;) {
@@ -992,6 +996,7 @@ static int open_image(mg_index* ix, const uint8_t* image, uint64_t L, int k, int
 struct Shapes {
   unsigned dual_blocks_per_sm, steal_chunk, first_tier, second_blocks_per_sm, finish_blocks_per_sm,
       long_blocks_per_sm, chunks, weighted_chunks, third_blocks_per_sm, pack_bases;
+  unsigned long_small_blocks_per_sm;  // the smaller long-read size: its occupancy (not tuned)
 };
 
 static int occupancy(const void* fn, int threads, size_t smem) {
@@ -1001,12 +1006,16 @@ static int occupancy(const void* fn, int threads, size_t smem) {
 }
 
 static Shapes shapes(const mg_index* ix) {
-  static int occ_dual = 0, occ_second = 0, occ_third = 0, occ_long = 0;
+  static int occ_dual = 0, occ_second = 0, occ_third = 0, occ_long = 0, occ_long_s = 0;
   if (!occ_dual) {
-    cudaFuncSetAttribute(k_classify_long, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LongSmem));
+    cudaFuncSetAttribute(k_classify_long<LongSmem, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(LongSmem));
+    cudaFuncSetAttribute(k_classify_long<LongSmemS, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(LongSmemS));
     occ_second = occupancy((const void*)k_classify_dual_list<128, kW2Warps>, kW2Warps * 32, 0);
     occ_third = occupancy((const void*)k_classify_dual_list<256, kW3Warps>, kW3Warps * 32, 0);
-    occ_long = occupancy((const void*)k_classify_long, kLgThreads, sizeof(LongSmem));
+    occ_long = occupancy((const void*)k_classify_long<LongSmem, 2>, kLgThreads, sizeof(LongSmem));
+    occ_long_s = occupancy((const void*)k_classify_long<LongSmemS, 4>, kLgThreads, sizeof(LongSmemS));
     occ_dual = occupancy((const void*)k_classify_dual, kW1Warps * 32, 0);
   }
   const mg_tuning& t = ix->tune;
@@ -1024,6 +1033,7 @@ static Shapes shapes(const mg_index* ix) {
   s.pack_bases = pick(t.pack_bases, 1, 1, 2);
   s.finish_blocks_per_sm = pick(t.finish_blocks_per_sm, 8, 1, 8);
   s.long_blocks_per_sm = pick(t.long_blocks_per_sm, (unsigned)occ_long, 1, (unsigned)occ_long);
+  s.long_small_blocks_per_sm = (unsigned)occ_long_s;
   s.chunks = pick(t.chunks, mg_index::kMaxChunks, 1, mg_index::kMaxChunks);
   s.weighted_chunks = pick(t.weighted_chunks, 1, 1, 2);
   return s;
@@ -1098,7 +1108,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
   }
   if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
       w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
-      w.ovf.alloc(6 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+      w.ovf.alloc(7 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
@@ -1107,7 +1117,8 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
 // 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovf0b | 60 work0b |
-// 64 n_ovf1b | 68 work of the long-read tier | 72 n_ovf0c | 76 work0c
+// 64 n_ovf1b | 68 work of the smaller long-read size | 72 n_ovf0c | 76 work0c | 80 n_ovf1c |
+// 84 work of the larger long-read size
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
                         bool plain, unsigned long long* chain, const ChainSync* cs) {
@@ -1141,6 +1152,9 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   uint32_t* ovf0c = w.ovf.as<uint32_t>() + 5 * (n + 4);  // the 128-posting tier's leftovers
   unsigned* n_ovf0c = (unsigned*)(ctr + 72);
   unsigned* work0c = (unsigned*)(ctr + 76);
+  uint32_t* ovf1c = w.ovf.as<uint32_t>() + 6 * (n + 4);  // the smaller long-read size's leftovers
+  unsigned* n_ovf1c = (unsigned*)(ctr + 80);
+  unsigned* work_long2 = (unsigned*)(ctr + 84);
   StageDev sd;
   sd.stage = w.stage.as<mg_candidate>();
   sd.arena = w.arena.as<mg_candidate>();
@@ -1154,7 +1168,10 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   static bool attr_set = false;
   if (!attr_set) {
     CU(cudaFuncSetAttribute(k_classify_block<kB2Threads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l2.total));
-    CU(cudaFuncSetAttribute(k_classify_long, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LongSmem)));
+    CU(cudaFuncSetAttribute(k_classify_long<LongSmem, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(LongSmem)));
+    CU(cudaFuncSetAttribute(k_classify_long<LongSmemS, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sizeof(LongSmemS)));
     attr_set = true;
   }
   const bool tm = ix->timing && ix->events_made;
@@ -1202,8 +1219,10 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
       k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, w.side>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[3], w.side));
-      k_classify_long<<<sh.long_blocks_per_sm * sms, kLgThreads, sizeof(LongSmem), w.side>>>(
-          ix->dix, b, sd, b.ovf1, b.n_ovf1, work_long, ovf1b, n_ovf1b);
+      k_classify_long<LongSmemS, 4><<<sh.long_small_blocks_per_sm * sms, kLgThreads, sizeof(LongSmemS), w.side>>>(
+          ix->dix, b, sd, b.ovf1, b.n_ovf1, work_long, ovf1c, n_ovf1c);
+      k_classify_long<LongSmem, 2><<<sh.long_blocks_per_sm * sms, kLgThreads, sizeof(LongSmem), w.side>>>(
+          ix->dix, b, sd, ovf1c, n_ovf1c, work_long2, ovf1b, n_ovf1b);
       k_classify_block<kB2Threads><<<(unsigned)sms, kB2Threads, l2.total, w.side>>>(
           ix->dix, b, sd, ovf1b, n_ovf1b, b.work2, b.ovf2, b.n_ovf2, nullptr, l2, c2, 0);
       if (tm) CU(cudaEventRecord(ix->ev[4], w.side));
@@ -1280,6 +1299,16 @@ int error_status(int err) {
 constexpr uint64_t kChunkReads = 65536;
 constexpr int kRunWhole = 1;
 
+// Threads of the packed upload's pool: one per CPU this process may run on, at most 32 (a thread
+// packs at about the rate one core reads memory, 5-10 GB/s).
+static int pack_threads() {
+  cpu_set_t set;
+  int n = 0;
+  if (sched_getaffinity(0, sizeof(set), &set) == 0) n = CPU_COUNT(&set);
+  if (n <= 0) n = (int)std::thread::hardware_concurrency();
+  return std::max(1, std::min(32, n));
+}
+
 // Batched form with host buffers, in chunks: chunk i's offsets and bases are copied on the index's h2d stream
 // while chunk i-1 is classified on its compute stream, and chunk i's read results go back on the
 // d2h stream while chunk i+1 is classified. The chunks share the device output: the compaction
@@ -1334,7 +1363,7 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   const uint64_t pack_need = n_bases / 4 + 64 * (uint64_t)(nc + 1), exc_need = n_bases / 32 + 4096 * (uint64_t)nc;
   if (pack) {
     if (!ix->pack_pool)
-      ix->pack_pool = new PackPool((int)std::min(16u, std::max(1u, std::thread::hardware_concurrency())));
+      ix->pack_pool = new PackPool(pack_threads());
     if (ix->h_pack_cap < pack_need) {
       if (ix->h_pack) cudaFreeHost(ix->h_pack);
       ix->h_pack = nullptr;

@@ -1,6 +1,8 @@
-// Long-read tier: reads longer than the warp tiers take (up to kLgQ bases), one block of
-// kLgThreads threads per read, both strands in turn, over reads taken from a list by work
-// stealing.
+// Long-read tier: reads longer than the warp tiers take, one block of kLgThreads threads per
+// read, both strands in turn, over reads taken from a list by work stealing. Two sizes: reads up
+// to kLsQ bases with up to kLsE postings per strand in a block of about 51 KB of shared memory
+// (four blocks per SM), then what they hand on, up to kLgQ bases and kLgE postings, in blocks of
+// about 105 KB (two per SM).
 //
 // The general path (process_strand, mg_kernels.cuh) sorts every posting of a strand twice:
 // by (refID, found index) for the occurrence filter and again, with the postings it dropped
@@ -27,6 +29,8 @@ constexpr int kLgThreads = 256;
 constexpr int kLgQ = 20480;     // longest read (the config's 20 kb reads)
 constexpr int kLgSeeds = 2047;  // seeds per strand (found index and seed index take 11 bits each)
 constexpr int kLgE = 4096;      // postings per strand
+constexpr int kLsQ = 8192;      // the smaller size: longest read
+constexpr int kLsE = 2048;      // the smaller size: postings per strand
 constexpr int kLgK = 1024;      // kept postings per strand
 constexpr int kLgC = 64;        // scored candidates per strand
 constexpr int kLgRT = 128;      // table of kept references (at most half of it used)
@@ -35,19 +39,27 @@ constexpr uint32_t kLgEmpty = 0xFFFFFFFFu;
 // Dynamic shared memory of one block. From the compaction on, the hash set holds the sort keys
 // (kA: kLgK uint64, kB: kLgK uint32), p_ref and p_pos the per-entry scratch X and Y, and p_fj
 // the coverage bitmap.
-struct alignas(16) LongSmem {
-  uint32_t hs[2 * kLgE];      // (refID << 11 | found index) set, open addressing
-  uint32_t p_ref[kLgE];       // the strand's postings in seed order
-  uint32_t p_pos[kLgE];
-  uint32_t p_fj[kLgE];        // found index | seed index << 11 | 1 << 31 for the pair's first posting
+template <int Q, int E>
+struct alignas(16) LongSmemT {
+  static constexpr int kQ = Q, kE = E;
+  uint32_t hs[2 * E];         // (refID << 11 | found index) set, open addressing
+  uint32_t p_ref[E];          // the strand's postings in seed order
+  uint32_t p_pos[E];
+  uint32_t p_fj[E];           // found index | seed index << 11 | 1 << 31 for the pair's first posting
   uint32_t rt[kLgRT];         // kept references
   mg_candidate cb[2][kLgC];   // scored candidates of the two strands
   RedTmp<kLgThreads> red;
   uint32_t n_kept, n_rt;
-  uint8_t q[kLgQ];            // strand bases
+  uint32_t scored[kLgC / 32];  // candidates with a score (bit per candidate)
+  uint32_t n_sc;
+  float hi;
+  uint8_t q[Q];               // strand bases
+  static_assert(kLgK * 12 <= 2 * E * 4 && Q / 32 + 1 <= E && 4 * kLgThreads <= 2 * E, "aliased regions");
 };
-static_assert(2 * sizeof(LongSmem) + 2048 <= 233472, "two blocks per SM");
-static_assert(kLgK * 12 <= 2 * kLgE * 4 && kLgQ / 32 + 1 <= kLgE, "aliased regions");
+using LongSmem = LongSmemT<kLgQ, kLgE>;       // two blocks per SM
+using LongSmemS = LongSmemT<kLsQ, kLsE>;      // four blocks per SM
+static_assert(2 * (sizeof(LongSmem) + 1024) <= 233472, "two blocks per SM");
+static_assert(4 * (sizeof(LongSmemS) + 1024) <= 233472, "four blocks per SM");
 
 __device__ __forceinline__ uint32_t lg_mix(uint32_t x) { return (x * 2654435761u) ^ (x >> 15); }
 
@@ -76,10 +88,12 @@ __device__ __forceinline__ bool lg_insert(uint32_t* set, uint32_t mask, uint32_t
   return false;
 }
 
-// One strand of a read (raw bytes, L <= kLgQ) on the whole block. Same contract as
+// One strand of a read (raw bytes, L <= SM::kQ) on the whole block. Same contract as
 // process_strand: kStrandOverflow hands the read to the block tier.
-__device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, int strand, LongSmem& S, int* err,
+template <class SM>
+__device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, int strand, SM& S, int* err,
                            uint32_t* n_out, float* highest) {
+  constexpr int kE = SM::kE;
   constexpr int G = kLgThreads;
   const int tid = threadIdx.x;
   const uint32_t k = (uint32_t)ix.k, step = (uint32_t)ix.step;
@@ -126,11 +140,11 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
       }
       found = (cnt > 0 || h == ix.empty_hash) ? 1u : 0u;
     }
-    const uint32_t x = cnt > (uint32_t)kLgE ? (uint32_t)kLgE + 1 : cnt;
+    const uint32_t x = cnt > (uint32_t)kE ? (uint32_t)kE + 1 : cnt;
     uint32_t fr, er;
     const uint32_t fi = grp_excl_sum<G>(found, red, &fr);
     const uint32_t ei = grp_excl_sum<G>(x, red, &er);
-    if (ne + er > (uint32_t)kLgE) return kStrandOverflow;  // group-uniform
+    if (ne + er > (uint32_t)kE) return kStrandOverflow;  // group-uniform
     const uint32_t e = ne + ei, fj = (nf + fi) | (j << 11);
     uint32_t t0 = 0;
     if (ix.slots) {
@@ -150,15 +164,36 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
       put(6, v3.z, v3.w);
       t0 = kSlotPosts;
     }
-    for (uint32_t t = t0; t < cnt; t++) {
-      const uint2 p = __ldg(ix.post + o0 + t);
-      S.p_ref[e + t] = p.x;
-      S.p_pos[e + t] = p.y;
-      S.p_fj[e + t] = fj;
+    // the postings past the slot's (all of them without slots), a warp per seed with its lanes on
+    // consecutive postings: each seed's (offset, count, start, fj) goes to the hash set's space,
+    // unused until step 2 (the barriers of the next group's sums order its reuse)
+    uint32_t* o0S = S.hs;
+    uint32_t* cntS = S.hs + G;
+    uint32_t* eS = S.hs + 2 * G;
+    uint32_t* fjS = S.hs + 3 * G;
+    o0S[tid] = o0;
+    cntS[tid] = cnt;
+    eS[tid] = e;
+    fjS[tid] = fj;
+    __syncthreads();
+    {
+      const uint32_t gn = min((uint32_t)G, ns - j0), lane = (uint32_t)tid & 31u;
+      for (uint32_t sd = (uint32_t)tid >> 5; sd < gn; sd += G / 32) {
+        const uint32_t c = cntS[sd];
+        if (c <= t0) continue;  // warp-uniform
+        const uint32_t o = o0S[sd], es = eS[sd], f = fjS[sd];
+        for (uint32_t t = t0 + lane; t < c; t += 32) {
+          const uint2 p = __ldg(ix.post + o + t);
+          S.p_ref[es + t] = p.x;
+          S.p_pos[es + t] = p.y;
+          S.p_fj[es + t] = f;
+        }
+      }
     }
     nf += fr;
     ne += er;
   }
+  __syncthreads();  // the postings in place before step 2 clears the hash set
   if (ne == 0) return kStrandOk;  // nothing found: the reference skips the strand
   // 2. occurrence filter: the (refID, found index) set
   uint32_t hsz = 64;
@@ -280,69 +315,109 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
       if (rhead(i) && Y[i] == M) kB[at++] = (uint32_t)i;  // kB's query positions are walked by now
   }
   __syncthreads();
-  uint32_t* cov = S.p_fj;
+  // 7. scores, a warp per candidate (Analyser.cpp:2490-2540, MatrixCPU.cpp:18-214): the candidate's
+  //    reference segment [sa, sb) of the sorted keys, its walked runs' lengths summed (sc) and summed
+  //    as triangles (sr), the query bases they cover counted in the warp's own bitmap; a candidate
+  //    whose runs all fell short of k keeps Score -2 and is not scored. Then the scored ones in
+  //    ascending refID, and the highest relative score in that order.
+  if (n_cand > (uint32_t)kLgC) return kStrandOverflow;  // group-uniform (n_rt bounds it first)
   const uint32_t nw = (L + 31) / 32;
-  uint32_t n_sc = 0;
-  float hi = -1.0f;
-  for (uint32_t c = 0; c < n_cand; c++) {
-    const int sa = (int)kB[c];
-    const uint32_t ref = refA(sa);
-    uint32_t first = (uint32_t)T2;
-    for (int i = sa + 1 + tid; i < T2; i += G)
-      if (refA(i) != ref) {
-        first = (uint32_t)i;
-        break;
+  const uint32_t lane = (uint32_t)tid & 31u, warp = (uint32_t)tid >> 5;
+  const uint32_t n_warps = min((uint32_t)(G / 32), (uint32_t)SM::kE / nw);  // bitmaps fit p_fj
+  if (tid < kLgC / 32) S.scored[tid] = 0;
+  __syncthreads();
+  mg_candidate* out = S.cb[strand];
+  if (warp < n_warps) {
+    uint32_t* cov = S.p_fj + warp * nw;
+    for (uint32_t c = warp; c < n_cand; c += n_warps) {
+      const int sa = (int)kB[c];
+      const uint32_t ref = refA(sa);
+      uint32_t first = (uint32_t)T2;
+      for (int i = sa + 1 + (int)lane; i < T2; i += 32)
+        if (refA(i) != ref) {
+          first = (uint32_t)i;
+          break;
+        }
+      const int sb = (int)__reduce_min_sync(0xFFFFFFFFu, first);
+      uint32_t sc = 0;
+      uint64_t sr = 0;
+      for (int i = sa + (int)lane; i < sb; i += 32) {
+        const uint32_t z = X[i];
+        if (z) {
+          const uint64_t t = z & 0xFFFFu;
+          sc += (uint32_t)t;
+          sr += (t * (t + 1)) / 2;
+        }
       }
-    const int sb = (int)(uint32_t)(~grp_max_u64<G>(~(uint64_t)first, red));  // group min
-    uint64_t sc = 0, sr = 0;
-    for (int i = sa + tid; i < sb; i += G) {
-      const uint32_t z = X[i];
-      if (z) {
-        const uint64_t t = z & 0xFFFFu;
-        sc += t;
-        sr += (t * (t + 1)) / 2;
+      sc = __reduce_add_sync(0xFFFFFFFFu, sc);  // at most kLgK runs of < 2^16 bases each
+      for (int o = 16; o; o >>= 1) sr += __shfl_xor_sync(0xFFFFFFFFu, sr, o);
+      if (sc == 0) continue;  // warp-uniform: Score stays -2
+      for (uint32_t w = lane; w < nw; w += 32) cov[w] = 0;
+      __syncwarp();
+      for (int i = sa + (int)lane; i < sb; i += 32) {
+        const uint32_t z = X[i];
+        if (!z) continue;
+        const uint32_t a = z >> 16, bnd = a + (z & 0xFFFFu);
+        for (uint32_t wd = a >> 5; wd <= (bnd - 1) >> 5; wd++) {
+          const uint32_t w0 = wd * 32;
+          const uint32_t lo = a > w0 ? a : w0, up = bnd < w0 + 32 ? bnd : w0 + 32;
+          const uint32_t n = up - lo;
+          atomicOr(&cov[wd], (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0));
+        }
       }
+      __syncwarp();
+      uint32_t hits = 0;
+      for (uint32_t w = lane; w < nw; w += 32) hits += __popc(cov[w]);
+      hits = __reduce_add_sync(0xFFFFFFFFu, hits);
+      if (lane == 0) {
+        float score, pct;
+        final_score(sr, (uint64_t)sc, hits, L, &score, &pct);
+        const float rel = relative_score(ix, __uint2float_rn(L), __uint2float_rn(ix.ref_len[ref]), score, err);
+        out[c] = mg_candidate{ref, rel, score, pct};
+        atomicOr(&S.scored[c >> 5], 1u << (c & 31u));
+      }
+      __syncwarp();  // the bitmap's next clear after this candidate's count
     }
-    for (uint32_t w = tid; w < nw; w += G) cov[w] = 0;
-    sc = grp_sum_u64<G>(sc, red);  // its barriers order the clear before the marks below
-    sr = grp_sum_u64<G>(sr, red);
-    if (sc == 0) continue;  // Score stays -2
-    for (int i = sa + tid; i < sb; i += G) {
-      const uint32_t z = X[i];
-      if (!z) continue;
-      const uint32_t a = z >> 16, bnd = a + (z & 0xFFFFu);
-      for (uint32_t wd = a >> 5; wd <= (bnd - 1) >> 5; wd++) {
-        const uint32_t w0 = wd * 32;
-        const uint32_t lo = a > w0 ? a : w0, up = bnd < w0 + 32 ? bnd : w0 + 32;
-        const uint32_t n = up - lo;
-        atomicOr(&cov[wd], (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0));
-      }
-    }
-    __syncthreads();
-    uint32_t hits = 0;
-    for (uint32_t w = tid; w < nw; w += G) hits += __popc(cov[w]);
-    hits = (uint32_t)grp_sum_u64<G>(hits, red);
-    float score, pct;
-    final_score(sr, sc, hits, L, &score, &pct);
-    const float rel = relative_score(ix, __uint2float_rn(L), __uint2float_rn(ix.ref_len[ref]), score, err);
-    if (n_sc >= (uint32_t)kLgC) return kStrandOverflow;
-    if (tid == 0) S.cb[strand][n_sc] = mg_candidate{ref, rel, score, pct};
-    n_sc++;
-    if (rel > hi) hi = rel;
   }
   __syncthreads();
+  if (warp == 0) {  // in place: a scored candidate only moves down, after its chunk is read
+    uint32_t n_sc = 0;
+    for (uint32_t c0 = 0; c0 < n_cand; c0 += 32) {
+      const uint32_t c = c0 + lane;
+      const bool ok = c < n_cand && ((S.scored[c >> 5] >> (c & 31u)) & 1u);
+      mg_candidate v{};
+      if (ok) v = out[c];
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
+      __syncwarp();
+      if (ok) out[n_sc + __popc(m & ((1u << lane) - 1u))] = v;
+      n_sc += __popc(m);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      float hi = -1.0f;
+      for (uint32_t i = 0; i < n_sc; i++)
+        if (out[i].rel > hi) hi = out[i].rel;
+      S.n_sc = n_sc;
+      S.hi = hi;
+    }
+  }
+  __syncthreads();
+  const uint32_t n_sc = S.n_sc;
+  const float hi = S.hi;
+  __syncthreads();  // S.n_sc and S.hi read before the next strand writes them
   *n_out = n_sc;
   *highest = hi;
   return kStrandOk;
 }
 
 // Both strands of read r, the strand merge and the staging write; false when the read must go
-// to the block tier.
-__device__ bool process_read_long(const DevIndex& ix, const BatchDev& b, uint32_t r, LongSmem& S, mg_candidate* stage,
+// to the next tier.
+template <class SM>
+__device__ bool process_read_long(const DevIndex& ix, const BatchDev& b, uint32_t r, SM& S, mg_candidate* stage,
                                   mg_candidate* arena, uint64_t arena_cap, unsigned long long* arena_n, int* errw) {
   const uint64_t o0 = b.offs[r];
   const uint64_t Lr = b.offs[r + 1] - o0;
-  if (Lr > (uint64_t)kLgQ || ix.n_refs > (1u << 21)) return false;  // keys hold refID << 11
+  if (Lr > (uint64_t)SM::kQ || ix.n_refs > (1u << 21)) return false;  // keys hold refID << 11
   const uint32_t L = (uint32_t)Lr;
   const uint8_t* raw = b.bases + o0;
   int err = 0;
@@ -350,7 +425,7 @@ __device__ bool process_read_long(const DevIndex& ix, const BatchDev& b, uint32_
   float h[2] = {-1.0f, -1.0f};
   int st = long_strand(ix, raw, L, 0, S, &err, &n[0], &h[0]);
   if (st != kStrandBad && st != kStrandOverflow) st = long_strand(ix, raw, L, 1, S, &err, &n[1], &h[1]);
-  if (err & kErrInternal) atomicOr(errw, kErrInternal);  // any thread's: the probes record it per thread
+  if (err) atomicOr(errw, err);  // any thread's: the probes and the scoring lanes record bits per thread
   if (st == kStrandOverflow) return false;
   if (threadIdx.x == 0)
     write_read_result_s(b, r, st == kStrandBad, n[0], n[1], h[0], h[1], S.cb[0], S.cb[1], stage, arena, arena_cap,

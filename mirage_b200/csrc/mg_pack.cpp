@@ -44,34 +44,36 @@ void pack_scalar(const uint8_t* src, uint64_t a, uint64_t b, uint8_t* dst, std::
   }
 }
 
+// 128 bases per step: each byte's code c, then its validity as (byte | 0x20) == "acgt"[c] (a byte
+// passes exactly when it is one of A, C, G, T in either case: those are the only bytes whose
+// lower-case form is a, c, g or t, and each maps to its own letter), one branch per step; the codes
+// of 4 consecutive bytes summed into one byte (c0 + 4 c1 + 16 c2 + 64 c3) per 32-bit lane, and
+// the four vectors' lanes narrowed and put in order for one 32-byte store.
 __attribute__((target("avx2"))) void pack_avx2(const uint8_t* src, uint64_t a, uint64_t b, uint8_t* dst,
                                                std::vector<uint64_t>& exc) {
-  const __m256i lo20 = _mm256_set1_epi8(0x20), ca = _mm256_set1_epi8('a'), cc = _mm256_set1_epi8('c'),
-                cg = _mm256_set1_epi8('g'), ct = _mm256_set1_epi8('t'), three = _mm256_set1_epi8(3);
-  const __m256i w14 = _mm256_set1_epi16(0x0401);  // bytes (1, 4): c0 + 4 c1 per 16 bits
+  const __m256i lo20 = _mm256_set1_epi8(0x20), three = _mm256_set1_epi8(3);
+  const __m256i letters = _mm256_setr_epi8('a', 'c', 'g', 't', 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 'a', 'c', 'g', 't',
+                                           0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
+  const __m256i w14 = _mm256_set1_epi16(0x0401);       // bytes (1, 4): c0 + 4 c1 per 16 bits
   const __m256i w116 = _mm256_set1_epi32(0x00100001);  // halves (1, 16): + 16 (c2 + 4 c3)
-  // byte 0 of each 32-bit lane to the low 4 bytes of each 128-bit half
-  const __m256i gather = _mm256_setr_epi8(0, 4, 8, 12, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, 0, 4, 8, 12, -1,
-                                          -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1);
+  const __m256i order = _mm256_setr_epi32(0, 4, 1, 5, 2, 6, 3, 7);
   uint64_t i = a;
-  for (; i + 32 <= b; i += 32) {
-    const __m256i v = _mm256_loadu_si256((const __m256i*)(src + i));
-    const __m256i l = _mm256_or_si256(v, lo20);
-    const __m256i ok = _mm256_or_si256(_mm256_or_si256(_mm256_cmpeq_epi8(l, ca), _mm256_cmpeq_epi8(l, cc)),
-                                       _mm256_or_si256(_mm256_cmpeq_epi8(l, cg), _mm256_cmpeq_epi8(l, ct)));
-    const uint32_t m = (uint32_t)_mm256_movemask_epi8(ok);
-    if (m != 0xFFFFFFFFu) {
-      for (uint32_t t = 0; t < 32; t++)
-        if (!((m >> t) & 1u)) exc.push_back(((i + t) << 8) | src[i + t]);
+  for (; i + 128 <= b; i += 128) {
+    __m256i p[4], ok = _mm256_set1_epi8(-1);
+    for (int v = 0; v < 4; v++) {
+      const __m256i x = _mm256_loadu_si256((const __m256i*)(src + i + 32 * v));
+      // per-byte codes: the 16-bit shifts carry bits across bytes only above bit 1, which & 3 drops
+      const __m256i c = _mm256_and_si256(_mm256_xor_si256(_mm256_srli_epi16(x, 1), _mm256_srli_epi16(x, 2)), three);
+      ok = _mm256_and_si256(ok, _mm256_cmpeq_epi8(_mm256_or_si256(x, lo20), _mm256_shuffle_epi8(letters, c)));
+      p[v] = _mm256_madd_epi16(_mm256_maddubs_epi16(c, w14), w116);  // one packed byte per 32-bit lane
     }
-    // per-byte codes: the 16-bit shifts carry bits across bytes only above bit 1, which & 3 drops
-    const __m256i c = _mm256_and_si256(_mm256_xor_si256(_mm256_srli_epi16(v, 1), _mm256_srli_epi16(v, 2)), three);
-    const __m256i p16 = _mm256_maddubs_epi16(c, w14);    // c0 + 4 c1
-    const __m256i p32 = _mm256_madd_epi16(p16, w116);   // (c0 + 4 c1) + 16 (c2 + 4 c3)
-    const __m256i g = _mm256_shuffle_epi8(p32, gather);  // 4 bytes per 128-bit half
-    const uint32_t lo = (uint32_t)_mm256_extract_epi32(g, 0), hi = (uint32_t)_mm256_extract_epi32(g, 4);
-    const uint64_t out = (uint64_t)lo | ((uint64_t)hi << 32);
-    std::memcpy(dst + (i >> 2), &out, 8);
+    if ((uint32_t)_mm256_movemask_epi8(ok) != 0xFFFFFFFFu) {
+      for (uint64_t t = i; t < i + 128; t++)
+        if (!is_base(src[t])) exc.push_back((t << 8) | src[t]);
+    }
+    // dwords after the two narrowings: [A0-3 B0-3 C0-3 D0-3 | A4-7 B4-7 C4-7 D4-7] -> A B C D
+    const __m256i n16 = _mm256_packus_epi16(_mm256_packus_epi32(p[0], p[1]), _mm256_packus_epi32(p[2], p[3]));
+    _mm256_storeu_si256((__m256i*)(dst + (i >> 2)), _mm256_permutevar8x32_epi32(n16, order));
   }
   pack_scalar(src, i, b, dst, exc);
 }
@@ -140,8 +142,8 @@ void PackPool::run(const std::function<void(int)>& job) {
 uint64_t pack_bases(PackPool& pool, const uint8_t* src, uint64_t n, uint8_t* dst, uint64_t* exc, uint64_t exc_cap,
                     uint64_t* n_exc) {
   const int T = pool.threads();
-  // slices of whole 32-byte blocks, so every slice but the last starts and ends on a packed byte
-  const uint64_t per = ((n + T - 1) / T + 31) / 32 * 32;
+  // slices of whole 128-byte steps, so every slice but the last starts and ends on a packed byte
+  const uint64_t per = ((n + T - 1) / T + 127) / 128 * 128;
   std::vector<std::vector<uint64_t>> local(T);
   pool.run([&](int t) {
     const uint64_t a = std::min(n, per * (uint64_t)t), b = std::min(n, a + per);

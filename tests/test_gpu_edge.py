@@ -369,3 +369,43 @@ def test_packed_upload_equals_plain_upload(golden):
         assert e.value.code == -6
     finally:
         ix.set_tuning()
+
+
+def test_long_reads_past_the_smaller_long_size(tmp_path):
+    """The long-read tier runs in two sizes: reads up to 8,192 bases with up to 2,048 postings per
+    strand in the smaller, what it hands on (to 20,480 bases and 4,096 postings) in the larger.
+    Reads of 8,191, 8,192 and 8,193 bases sit either side of the length bound; 6,000-base reads
+    whose even seed windows also lie in ten decoy references (occurrence runs of 1, never kept)
+    gather 2,049 to 4,096 postings on the forward strand, so the smaller size hands them to the
+    larger. Every result equals the oracle."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(53)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 30000)]
+    k, step, hlen, L = 31, 15, 17, 6000
+    starts = [0, 7000, 14000]
+    ns = (L - k + step - 1) // step
+    decoys = []
+    for _ in range(10):
+        parts = []
+        for s in starts:
+            for j in range(0, ns, 2):
+                parts.append(core[s + j * step:s + j * step + hlen])
+                parts.append(acgt[rng.integers(0, 4, 20)])
+        decoys.append(np.concatenate(parts))
+    refs = [core] + decoys + [acgt[rng.integers(0, 4, 10000)]]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))], k=k)
+    path = tmp_path / "decoys10.mhm"
+    image.tofile(path)
+    gix, oix = M.Index(image, k=k), O.Index(str(path), k=k)
+    heavy = [core[s:s + L].tobytes() for s in starts]
+    hashes = [O.lib().mgo_hash28(q[j * step:j * step + hlen], hlen) for q in heavy for j in range(ns)]
+    per_read = gix.bucket_sizes(np.array(hashes, np.uint32)).astype(np.int64).reshape(len(heavy), ns).sum(1)
+    assert (per_read > 2048).all() and (per_read <= 4096).all(), per_read
+    seqs = heavy + [h.lower() for h in heavy]
+    seqs += [core[20000:20000 + 8192].tobytes(), core[21000:21000 + 8193].tobytes(), core[20500:20500 + 8191].tobytes()]
+    r = check_against_oracle(gix, oix, seqs)
+    assert (r.reads["n_fwd"][:3] >= 1).all()
