@@ -51,9 +51,11 @@ LAUNCHES_PER_BATCH = 9
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_classify_dual launch on the
 # default workload (1,000,000 reads, scale 1.0): a constant from one ncu capture of this kernel,
 # not a measurement of this run
-DUAL_TRAFFIC_DEFAULT = 5_389_143_040 + 49_829_632
-DUAL_TRAFFIC_WHAT = ("DRAM bytes per k_classify_dual launch: a constant from one ncu capture of the kernel on "
-                     "this workload (dram__bytes_read.sum + dram__bytes_write.sum), not measured in this run")
+# dram__bytes_read.sum + dram__bytes_write.sum of k_classify_dual and of k_finish_dual, one launch each
+DUAL_TRAFFIC_DEFAULT = (2_986_232_832 + 47_951_616) + (357_686_528 + 63_106_304)
+DUAL_TRAFFIC_WHAT = ("DRAM bytes per step of k_classify_dual + k_finish_dual (the kernels of kernel_ms but the "
+                     "side tiers): a constant from one ncu capture of each on this workload "
+                     "(dram__bytes_read.sum + dram__bytes_write.sum), not measured in this run")
 
 
 def log(*a):
@@ -425,8 +427,10 @@ def main():
         args.reads = WORKLOADS[args.workload]["reads"]
     if args.cpu_sample is None:
         args.cpu_sample = WORKLOADS[args.workload]["cpu_sample"]
-    if args.workload != "uneven":
-        args.served_seconds = 0.0  # the served form is measured on the uneven workload (its request shape)
+    if args.workload not in ("uneven", "large"):
+        # the served form runs on the index of configuration 2 (its request stream) and of the large
+        # index stress; the plain and long workloads measure the batched and plain forms only
+        args.served_seconds = 0.0
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
