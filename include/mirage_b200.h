@@ -293,17 +293,17 @@ int mg_server_submit_into(mg_server* s, const mg_batch* batch, mg_result* out, u
  * MG_ERR_INVAL: the server reads directly only from ranges that it registered itself. Ranges
  * stay registered, and must stay allocated, until mg_server_destroy. */
 int mg_server_register_host(mg_server* s, const void* ptr, uint64_t len);
-/* Where the server's time went since mg_server_create (seconds; the server thread's phases sum
- * to its lifetime). */
+/* Where the server's time went since mg_server_create (seconds; the server thread's launch,
+ * device and idle times sum to its lifetime; the delivery thread's time is apart). */
 typedef struct {
   uint64_t steps, reads, requests;
   uint64_t ring_bytes;    /* bases that submit copied into the request ring */
   uint64_t direct_bytes;  /* bases copied to the device from registered caller memory */
   double submit_copy_s;   /* submit: copying requests into the ring, summed over the callers */
   double launch_s;        /* server thread: forming steps, host-to-device copies, launches */
-  double device_s;        /* server thread: waiting for steps and their result copies */
-  double deliver_s;       /* server thread: handing results to requests */
-  double idle_s;          /* server thread: waiting for requests */
+  double device_s;        /* server thread: draining finished steps (counters, candidate copies) */
+  double deliver_s;       /* delivery thread: handing results to requests */
+  double idle_s;          /* server thread: waiting for requests, a free step slot or a step to finish */
 } mg_server_stats;
 int mg_server_get_stats(mg_server* s, mg_server_stats* out);
 /* Non-blocking: returns 1 and fills out when the request is complete, 0 when not yet. */

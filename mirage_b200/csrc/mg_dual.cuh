@@ -171,7 +171,11 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
   if (!__any_sync(FULL, alive)) return kStrandOk;
   __syncwarp();
   const uint32_t keep_min = (uint32_t)(hs - 1);  // max(1, hs - 1), Analyser.cpp:2115
-  // kept postings compacted in gather order
+  // kept postings compacted in gather order: as one 64-bit key ref << 37 | pos << 5 | seed (the
+  // order of (ref, pos, seed): seeds < 32, positions < 2^32, references < 2^27) in the c arrays'
+  // first two rows, or, for an index of more references, as three words
+  const bool k64 = ix.n_refs <= (1u << 27);  // warp-uniform
+  unsigned long long* c_key = reinterpret_cast<unsigned long long*>(c_ref);  // c_ref and c_pos rows
   uint32_t T2 = 0;
   for (int s = 0; s < nslw; s++) {
     const uint32_t i = hl + 16 * s;
@@ -184,9 +188,14 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
     const uint32_t kb = half_bits(__ballot_sync(FULL, kp), sh);
     if (kp) {
       const uint32_t c = T2 + __popc(kb & ((1u << hl) - 1u));
-      c_ref[c] = e_ref[i];
-      c_pos[c] = e_pos[i];
-      c_j[c] = (fj >> 8) & 0xFFu;
+      const uint32_t jj = (fj >> 8) & 0xFFu;
+      if (k64) {
+        c_key[c] = ((unsigned long long)e_ref[i] << 37) | ((unsigned long long)e_pos[i] << 5) | jj;
+      } else {
+        c_ref[c] = e_ref[i];
+        c_pos[c] = e_pos[i];
+        c_j[c] = jj;
+      }
     }
     T2 += __popc(kb);
   }
@@ -200,11 +209,21 @@ __device__ int dual_strands(const DevIndex& ix, uint32_t L, DualSmemT<Cap>& S, u
   for (int s = 0; s < nkw; s++) {
     const uint32_t c = hl + 16 * s;
     if (c < T2) {
-      const uint32_t r = c_ref[c], p = c_pos[c], j = c_j[c];
-      uint32_t rk = 0;
-      for (uint32_t i = 0; i < T2; i++) {
-        const uint32_t rr = c_ref[i], pp = c_pos[i], jj = c_j[i];
-        rk += (rr < r || (rr == r && (pp < p || (pp == p && jj < j)))) ? 1u : 0u;
+      uint32_t r, p, j, rk = 0;
+      if (k64) {
+        const unsigned long long key = c_key[c];
+        for (uint32_t i = 0; i < T2; i++) rk += c_key[i] < key ? 1u : 0u;
+        r = (uint32_t)(key >> 37);
+        p = (uint32_t)(key >> 5);
+        j = (uint32_t)key & 31u;
+      } else {
+        r = c_ref[c];
+        p = c_pos[c];
+        j = c_j[c];
+        for (uint32_t i = 0; i < T2; i++) {
+          const uint32_t rr = c_ref[i], pp = c_pos[i], jj = c_j[i];
+          rk += (rr < r || (rr == r && (pp < p || (pp == p && jj < j)))) ? 1u : 0u;
+        }
       }
       s_ref[rk] = r;
       s_pos[rk] = p;

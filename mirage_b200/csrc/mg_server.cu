@@ -93,6 +93,8 @@ struct Slot {
   bool busy = false;      // from carving until its results are delivered
   int launch_rc = 0;
   int drain_rc = 0;       // the step's status after the device part of draining
+  mg_server* owner = nullptr;
+  std::atomic<bool> device_done{false};  // the step's device work and read-result copy have finished
 };
 
 }  // namespace mg
@@ -202,6 +204,7 @@ static void carve_step(mg_server* sv, Slot& s) {
   }
   s.busy = true;
   s.launch_rc = MG_OK;
+  s.device_done = false;
 }
 
 // Split a step's parts into pieces of at most kPieceReads reads.
@@ -238,7 +241,7 @@ static void for_pieces(PackPool* pool, Slot& s, F&& fn) {
 // Copy a carved step's segments from the ring (or the caller's registered memory) and launch it on
 // the slot's stream (server lock not held: the segments' requests stay queued-or-running, so their
 // memory stays in place). The offsets, rebased into the step, are written by the launch workers.
-static void launch_step(mg_server* sv, Slot& s) {
+static void launch_step_work(mg_server* sv, Slot& s) {
   if (s.n == 0) return;
   make_pieces(s);
   uint64_t nb = 0;
@@ -281,7 +284,27 @@ static void launch_step(mg_server* sv, Slot& s) {
     s.launch_rc = MG_ERR_CUDA;
 }
 
-// Wait for a launched step and bring its results to the slot's pinned buffers (server thread;
+// Host function enqueued after a step's work: marks the step done on the device and wakes the
+// server thread (no CUDA call here). The notify happens under the lock, so once the lock is
+// released this function touches the server no more (the server may then be destroyed).
+static void CUDART_CB step_done(void* p) {
+  Slot* s = static_cast<Slot*>(p);
+  mg_server* sv = s->owner;
+  std::lock_guard<std::mutex> lk(sv->mu);
+  s->device_done = true;
+  sv->cv_work.notify_one();
+}
+
+static void launch_step(mg_server* sv, Slot& s) {
+  launch_step_work(sv, s);
+  if (s.launch_rc == MG_OK && s.n) {
+    if (cudaLaunchHostFunc(s.st, step_done, &s) == cudaSuccess) return;
+    s.launch_rc = set_error(MG_ERR_CUDA, "cudaLaunchHostFunc");
+  }
+  s.device_done = true;  // nothing to wait for (drain_device synchronises the stream on an error)
+}
+
+// Bring a step that has finished on the device to the slot's pinned buffers (server thread;
 // lock not held). The step's status goes to s.drain_rc for the delivery thread.
 static void drain_device(mg_server* sv, Slot& s) {
   const auto t_wait = Clock::now();
@@ -435,15 +458,19 @@ static bool slot_free_now(const mg_server* sv) {
   return false;
 }
 
-// Server thread: carves and launches steps into free slots and waits for each launched step in
-// turn; the delivery thread then hands its results out and frees the slot.
+// Server thread: carves and launches steps into free slots, and drains the oldest launched step
+// once it has finished on the device; the delivery thread then hands its results out and frees
+// the slot. It sleeps until one of those can happen: work and a free slot (a delivery freed
+// one, or a request came), or the oldest step done (its host function).
 static void server_loop(mg_server* sv) {
   cudaSetDevice(sv->ix->device);
   std::unique_lock<std::mutex> lk(sv->mu);
+  auto oldest_done = [&] { return !sv->in_flight.empty() && sv->slot[sv->in_flight.front()].device_done; };
   for (;;) {
     const auto t_idle = Clock::now();
     sv->cv_work.wait(lk, [&] {
-      return sv->stop || (!sv->queue.empty() && slot_free_now(sv)) || !sv->in_flight.empty();
+      return (sv->stop && sv->in_flight.empty()) || (!sv->stop && !sv->queue.empty() && slot_free_now(sv)) ||
+             oldest_done();
     });
     sv->ns_idle += ns_since(t_idle);
     if (sv->stop && sv->in_flight.empty()) break;
@@ -460,8 +487,8 @@ static void server_loop(mg_server* sv) {
         lk.lock();
       }
     }
-    // wait for the oldest launched step, then pass it to the delivery thread
-    if (sv->in_flight.empty()) continue;
+    // drain the oldest launched step when it is done, then pass it to the delivery thread
+    if (!oldest_done()) continue;
     const int d = sv->in_flight.front();
     sv->in_flight.pop_front();
     lk.unlock();
@@ -519,6 +546,7 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
   }
   for (int i = 0; i < sv->n_slots; i++) {
     Slot& s = sv->slot[i];
+    s.owner = sv;
     if (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess ||
         slot_alloc(s, sv->step_reads, sv->step_bases, 16 * sv->step_reads + 1024) != MG_OK) {
       for (auto& t : sv->slot) slot_free(t);
