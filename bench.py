@@ -364,9 +364,10 @@ def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s:
     """Served form (mg_server_*): saturated throughput, then latency under Poisson arrivals at
     fractions of it. Native client threads (mirage_b200/libmg_loadgen.so) drive the server
     through the public C ABI: requests are contiguous slices of the host reads with log-uniform
-    sizes in [1, 50000] reads; each submit copies its request from host memory and the server
-    writes its results into the client's own buffers (mg_server_submit_into), inside the
-    measurement."""
+    sizes in [1, 50000] reads, whose pool is registered with the server (mg_server_register_host),
+    so each submit copies the request's offsets and the server copies its bases to the device
+    straight from the pool; the server writes the results into the client's own buffers
+    (mg_server_submit_into), inside the measurement."""
     import ctypes as C
 
     class Report(C.Structure):
@@ -380,6 +381,7 @@ def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s:
     offs = np.ascontiguousarray(offs, np.uint64)
     n = len(offs) - 1
     sv = M.Server(ix)
+    sv.register_host(bases)  # the reads' pool: requests' bases go to the device straight from it
 
     def run(rate: float, secs: float, depth: int, k: int) -> Report:
         rep = Report()
@@ -401,6 +403,8 @@ def served_bench(M, ix, bases: np.ndarray, offs: np.ndarray, seed: int, level_s:
                 "requests": "log-uniform 1..50000 reads, contiguous slices of the batch",
                 "clients": f"{clients} native threads (libmg_loadgen.so), closed loop 32 deep when saturated",
                 "results": "written by the server into each client's buffers (mg_server_submit_into)",
+                "bases": "the pool of reads registered with the server (mg_server_register_host): each request's "
+                         "bases copied to the device from it, its offsets through the request ring",
                 "arrivals": "Poisson (one process per client thread)", "seconds_per_level": level_s, "load": levels}
     finally:
         sv.close()

@@ -272,7 +272,7 @@ typedef struct {
   uint32_t max_requests;        /* concurrently tracked requests (0: default) */
   uint64_t device_budget;       /* bytes of device memory for request buffers (0: a quarter of the free memory) */
   uint32_t step_slots;          /* steps in flight at once, each with its own device buffers and stream
-                                 * (2-4; 0: 2) */
+                                 * (2-4; 0: 3) */
 } mg_server_config;
 
 int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out);
@@ -304,6 +304,7 @@ typedef struct {
   double device_s;        /* server thread: draining finished steps (counters, candidate copies) */
   double deliver_s;       /* delivery thread: handing results to requests */
   double idle_s;          /* server thread: waiting for requests, a free step slot or a step to finish */
+  double step_s;          /* summed over steps: from launch to the end of the step's device work */
 } mg_server_stats;
 int mg_server_get_stats(mg_server* s, mg_server_stats* out);
 /* Non-blocking: returns 1 and fills out when the request is complete, 0 when not yet. */

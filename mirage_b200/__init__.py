@@ -74,7 +74,7 @@ class _ServerConfig(C.Structure):
 class _ServerStats(C.Structure):
     _fields_ = [("steps", C.c_uint64), ("reads", C.c_uint64), ("requests", C.c_uint64), ("ring_bytes", C.c_uint64),
                 ("direct_bytes", C.c_uint64), ("submit_copy_s", C.c_double), ("launch_s", C.c_double),
-                ("device_s", C.c_double), ("deliver_s", C.c_double), ("idle_s", C.c_double)]
+                ("device_s", C.c_double), ("deliver_s", C.c_double), ("idle_s", C.c_double), ("step_s", C.c_double)]
 
 
 _lib = None

@@ -1456,9 +1456,11 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   if (rc) return rc;
   if (w.cands.alloc(std::max<uint64_t>(out->cand_cap, 1) * sizeof(mg_candidate)))
     return set_error(MG_ERR_OOM, "candidate buffer");
+  bool chunks_overflowed = false;
   if (!plain && n >= 2 * kChunkReads && shapes(ix).chunks > 1) {
     rc = classify_chunked(ix, w, batch, out);
     if (rc != kRunWhole) return rc;
+    chunks_overflowed = true;
   }
   cudaStream_t st = ix->stream;
   if (n) {
@@ -1476,6 +1478,10 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   if (rc) return rc;
   rc = error_status(c.err);
   if (rc) return rc;
+  // a chunk's staging arena ran out: the odd chunks' workspace, sized for one chunk, gets the
+  // arena the whole batch needed (no chunk needs more), so that batches like this one stay in
+  // chunks from now on (a failed allocation only leaves them on this path)
+  if (chunks_overflowed && ix->ws2.arena.alloc(w.arena.n)) cudaGetLastError();  // not sticky: clear it
   if (n) {
     CU(cudaMemcpyAsync(out->reads, w.reads.p, n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, st));
     if (total) CU(cudaMemcpyAsync(out->cands, w.cands.p, total * sizeof(mg_candidate), cudaMemcpyDeviceToHost, st));

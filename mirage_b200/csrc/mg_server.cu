@@ -95,6 +95,7 @@ struct Slot {
   int drain_rc = 0;       // the step's status after the device part of draining
   mg_server* owner = nullptr;
   std::atomic<bool> device_done{false};  // the step's device work and read-result copy have finished
+  std::chrono::steady_clock::time_point t_launch, t_done;  // launch start; end of the device work
 };
 
 }  // namespace mg
@@ -113,7 +114,7 @@ struct mg_server {
   std::map<uint64_t, std::unique_ptr<mg::Request>> live;   // every tracked request
   static constexpr int kMaxSlots = 4;
   mg::Slot slot[kMaxSlots];
-  int n_slots = 2;                  // step slots in use (mg_server_config.step_slots)
+  int n_slots = 3;                  // step slots in use (mg_server_config.step_slots)
   std::deque<int> in_flight;        // launched slots in launch order
   std::deque<int> to_deliver;       // drained slots in launch order, for the delivery thread
   std::condition_variable cv_deliver;
@@ -127,7 +128,7 @@ struct mg_server {
   std::vector<HostRange> host_ranges;  // page-locked by mg_server_register_host (under mu)
   // mg_server_get_stats
   std::atomic<uint64_t> n_steps{0}, n_reads{0}, n_requests{0}, ring_bytes{0}, direct_bytes{0};
-  std::atomic<uint64_t> ns_submit{0}, ns_launch{0}, ns_device{0}, ns_deliver{0}, ns_idle{0};
+  std::atomic<uint64_t> ns_submit{0}, ns_launch{0}, ns_device{0}, ns_deliver{0}, ns_idle{0}, ns_step{0};
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   bool stop = false;
@@ -291,11 +292,14 @@ static void CUDART_CB step_done(void* p) {
   Slot* s = static_cast<Slot*>(p);
   mg_server* sv = s->owner;
   std::lock_guard<std::mutex> lk(sv->mu);
+  s->t_done = Clock::now();
   s->device_done = true;
   sv->cv_work.notify_one();
 }
 
 static void launch_step(mg_server* sv, Slot& s) {
+  s.t_launch = Clock::now();
+  s.t_done = s.t_launch;
   launch_step_work(sv, s);
   if (s.launch_rc == MG_OK && s.n) {
     if (cudaLaunchHostFunc(s.st, step_done, &s) == cudaSuccess) return;
@@ -344,6 +348,8 @@ static void drain_device(mg_server* sv, Slot& s) {
       rc = set_error(MG_ERR_CUDA, "step results");
   }
   s.drain_rc = rc;
+  if (s.t_done > s.t_launch)
+    sv->ns_step += (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(s.t_done - s.t_launch).count();
   // the device budget follows the device's free memory, read at most every kBudgetRefresh (the
   // query is a driver call, too slow for every step)
   const auto now = Clock::now();
@@ -537,7 +543,7 @@ int mg_server_create(mg_index* ix, const mg_server_config* cfg, mg_server** out)
   sv->step_reads = reads;
   sv->step_bases = reads * 320;
   sv->max_requests = c.max_requests ? c.max_requests : 4096;
-  sv->n_slots = c.step_slots ? (int)std::min<uint32_t>(std::max<uint32_t>(c.step_slots, 2), mg_server::kMaxSlots) : 2;
+  sv->n_slots = c.step_slots ? (int)std::min<uint32_t>(std::max<uint32_t>(c.step_slots, 2), mg_server::kMaxSlots) : 3;
   // pinned ring for queued requests: (slots + 2) steps' worth of reads, at least 64 MB
   sv->ring.cap = std::max<uint64_t>(64ull << 20, (uint64_t)(sv->n_slots + 2) * (sv->step_bases + (sv->step_reads + 1) * 8));
   if (cudaMallocHost((void**)&sv->ring.base, sv->ring.cap) != cudaSuccess) {
@@ -736,6 +742,7 @@ int mg_server_get_stats(mg_server* sv, mg_server_stats* out) {
   out->device_s = sv->ns_device * 1e-9;
   out->deliver_s = sv->ns_deliver * 1e-9;
   out->idle_s = sv->ns_idle * 1e-9;
+  out->step_s = sv->ns_step * 1e-9;
   return MG_OK;
 }
 
