@@ -1,8 +1,8 @@
 // Long-read tier: reads longer than the warp tiers take, one block of kLgThreads threads per
 // read, both strands in turn, over reads taken from a list by work stealing. Two sizes: reads up
-// to kLsQ bases with up to kLsE postings per strand in a block of about 51 KB of shared memory
-// (four blocks per SM), then what they hand on, up to kLgQ bases and kLgE postings, in blocks of
-// about 105 KB (two per SM).
+// to kLsQ bases with up to kLsE postings and kLsK kept postings per strand in a block of about
+// 51 KB of shared memory (four blocks per SM), then what they hand on, up to kLgQ bases, kLgE
+// postings and kLgK kept postings, in blocks of about 105 KB (two per SM).
 //
 // The general path (process_strand, mg_kernels.cuh) sorts every posting of a strand twice:
 // by (refID, found index) for the occurrence filter and again, with the postings it dropped
@@ -31,17 +31,18 @@ constexpr int kLgSeeds = 2047;  // seeds per strand (found index and seed index 
 constexpr int kLgE = 4096;      // postings per strand
 constexpr int kLsQ = 8192;      // the smaller size: longest read
 constexpr int kLsE = 2048;      // the smaller size: postings per strand
-constexpr int kLgK = 1024;      // kept postings per strand
+constexpr int kLgK = 2048;      // kept postings per strand (the larger size)
+constexpr int kLsK = 1024;      // the smaller size: kept postings per strand
 constexpr int kLgC = 64;        // scored candidates per strand
 constexpr int kLgRT = 128;      // table of kept references (at most half of it used)
 constexpr uint32_t kLgEmpty = 0xFFFFFFFFu;
 
 // Dynamic shared memory of one block. From the compaction on, the hash set holds the sort keys
-// (kA: kLgK uint64, kB: kLgK uint32), p_ref and p_pos the per-entry scratch X and Y, and p_fj
+// (kA: K uint64, kB: K uint32), p_ref and p_pos the per-entry scratch X and Y, and p_fj
 // the coverage bitmap.
-template <int Q, int E>
+template <int Q, int E, int K>
 struct alignas(16) LongSmemT {
-  static constexpr int kQ = Q, kE = E;
+  static constexpr int kQ = Q, kE = E, kK = K;
   uint32_t hs[2 * E];         // (refID << 11 | found index) set, open addressing
   uint32_t p_ref[E];          // the strand's postings in seed order
   uint32_t p_pos[E];
@@ -54,10 +55,10 @@ struct alignas(16) LongSmemT {
   uint32_t n_sc;
   float hi;
   uint8_t q[Q];               // strand bases
-  static_assert(kLgK * 12 <= 2 * E * 4 && Q / 32 + 1 <= E && 4 * kLgThreads <= 2 * E, "aliased regions");
+  static_assert(K * 12 <= 2 * E * 4 && K <= E && Q / 32 + 1 <= E && 4 * kLgThreads <= 2 * E, "aliased regions");
 };
-using LongSmem = LongSmemT<kLgQ, kLgE>;       // two blocks per SM
-using LongSmemS = LongSmemT<kLsQ, kLsE>;      // four blocks per SM
+using LongSmem = LongSmemT<kLgQ, kLgE, kLgK>;   // two blocks per SM
+using LongSmemS = LongSmemT<kLsQ, kLsE, kLsK>;  // four blocks per SM
 static_assert(2 * (sizeof(LongSmem) + 1024) <= 233472, "two blocks per SM");
 static_assert(4 * (sizeof(LongSmemS) + 1024) <= 233472, "four blocks per SM");
 
@@ -237,12 +238,13 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
   if (S.n_rt > (uint32_t)kLgRT / 2) return kStrandOverflow;
   // 3. the kept references' postings, as (refID << 32 | position, query position) sort keys
   uint64_t* kA = reinterpret_cast<uint64_t*>(S.hs);
-  uint32_t* kB = S.hs + 2 * kLgK;
+  constexpr int kK = SM::kK;
+  uint32_t* kB = S.hs + 2 * kK;
   for (uint32_t i = tid; i < ne; i += G) {
     const uint32_t ref = S.p_ref[i];
     if (lg_contains(S.rt, kLgRT - 1, ref, err)) {
       const uint32_t t = atomicAdd(&S.n_kept, 1u);
-      if (t < (uint32_t)kLgK) {
+      if (t < (uint32_t)kK) {
         kA[t] = ((uint64_t)ref << 32) | S.p_pos[i];
         kB[t] = ((S.p_fj[i] >> 11) & 0x7FFu) * step;
       }
@@ -250,7 +252,7 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
   }
   __syncthreads();
   const int T2 = (int)S.n_kept;
-  if (T2 > kLgK) return kStrandOverflow;
+  if (T2 > kK) return kStrandOverflow;
   const int N = next_pow2(T2);
   for (int i = T2 + tid; i < N; i += G) {
     kA[i] = ~0ull;
@@ -349,7 +351,7 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
           sr += (t * (t + 1)) / 2;
         }
       }
-      sc = __reduce_add_sync(0xFFFFFFFFu, sc);  // at most kLgK runs of < 2^16 bases each
+      sc = __reduce_add_sync(0xFFFFFFFFu, sc);  // at most kK runs of < 2^16 bases each
       for (int o = 16; o; o >>= 1) sr += __shfl_xor_sync(0xFFFFFFFFu, sr, o);
       if (sc == 0) continue;  // warp-uniform: Score stays -2
       for (uint32_t w = lane; w < nw; w += 32) cov[w] = 0;

@@ -243,10 +243,11 @@ def test_chunked_batch_staging_overflow_runs_whole(tmp_path):
 
 def test_long_read_tier_and_its_hand_offs(tmp_path):
     """Reads of 400 bases to 20 kb on four identical references (every posting of a read's
-    true region kept four times) and one unrelated one: the long-read tier scores the reads
-    whose kept postings fit it (up to 1,024 per strand), hands longer ones to the block tier
-    (more kept postings) and to the global-memory tier (more than 4,096 postings per strand),
-    with errors and lowercase bases in some reads; every result equals the oracle's."""
+    true region kept four times) and one unrelated one: the long-read tier's smaller size scores
+    the reads whose kept postings fit it (up to 1,024 per strand), its larger size those up to
+    2,048 (4,000 and 6,000 bases), which hands longer ones to the block tier (12 kb: more kept
+    postings) and to the global-memory tier (20 kb: more than 4,096 postings per strand), with
+    errors and lowercase bases in some reads; every result equals the oracle's."""
     from oracle import oracle as O
 
     rng = np.random.default_rng(43)
