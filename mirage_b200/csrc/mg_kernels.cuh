@@ -77,31 +77,18 @@ __device__ __forceinline__ void bitonic_sort(uint64_t* kA, uint32_t* kB, int N) 
   }
 }
 
-// The first i in [0, n) with qb(i) != rb(i), else n. Sixteen comparisons at a time, each load
-// guarded only by the bound, so a group's loads do not wait on one another: a walk of k = 31
-// bases costs two memory round trips instead of one per base.
-template <class QB, class RB>
-__device__ __forceinline__ uint32_t first_mismatch(QB qb, RB rb, uint32_t n) {
-  for (uint32_t i0 = 0; i0 < n; i0 += 16) {
-    uint32_t m = 0;
-#pragma unroll
-    for (uint32_t i = 0; i < 16; i++)
-      if (i0 + i < n && qb(i0 + i) != rb(i0 + i)) m |= 1u << i;
-    if (m) return i0 + (uint32_t)__ffs(m) - 1u;
-  }
-  return n;
-}
-
 // Head walk (MatrixCPU.cpp:116-171): the query byte Start.Q-1-j is compared with the reference
 // byte Start.Ref-j; the walk stops at the first mismatch j, or after a match at j when
-// Start.Q-1-j, Start.Ref-j or headSize-1-j reaches 0, with the count j in both cases: the first
-// mismatch below jb = min(Start.Q-1, headSize-1), else jb.
+// Start.Q-1-j, Start.Ref-j or headSize-1-j reaches 0, with the count j in both cases.
 __device__ __forceinline__ uint32_t head_walk(const uint8_t* q, const uint8_t* rs, uint32_t sq, uint32_t sr, uint32_t k) {
   if (sq == 0) return 0;
   uint32_t hs = sr < k ? sr : k;
   if (hs == 0) return 0;
-  const uint32_t jb = sq - 1 < hs - 1 ? sq - 1 : hs - 1;
-  return first_mismatch([&](uint32_t j) { return q[sq - 1 - j]; }, [&](uint32_t j) { return rs[sr - j]; }, jb);
+  uint32_t jb = sq - 1 < hs - 1 ? sq - 1 : hs - 1;
+  for (uint32_t j = 0;; j++) {
+    if (q[sq - 1 - j] != rs[sr - j]) return j;
+    if (j == jb) return j;
+  }
 }
 
 // Tail walk (MatrixCPU.cpp:93-112): matches from Last onwards, bounded by the read end, the
@@ -112,7 +99,9 @@ __device__ __forceinline__ uint32_t tail_walk(const uint8_t* q, const uint8_t* r
   uint32_t lim = rlen - lr;
   if (k < lim) lim = k;
   if (L - lq < lim) lim = L - lq;
-  return first_mismatch([&](uint32_t i) { return q[lq + i]; }, [&](uint32_t i) { return rs[lr + i]; }, lim);
+  uint32_t i = 0;
+  while (i < lim && q[lq + i] == rs[lr + i]) i++;
+  return i;
 }
 
 // One strand. Returns kStrandOverflow when the read does not fit the workspace caps (the

@@ -170,8 +170,8 @@ constexpr int kFinRecCap = 128;              // run records a warp walks togethe
 
 // The head and tail walks of one run record x (head_walk, tail_walk) on the strand's bases, read
 // from the batch (raw, L bytes): forward in upper case, the reverse complement backwards through
-// the complement table. Returns the run's query start << 16 | its extended length T, or 0 when
-// T < k.
+// the complement table; the tail four bytes at a time while the window has four left. Returns the
+// run's query start << 16 | its extended length T, or 0 when T < k.
 __device__ __forceinline__ uint32_t walk_record(const DevIndex& ix, const uint8_t* comp, const uint8_t* raw, uint32_t L,
                                                 int strand, const mg_candidate& x, uint32_t k, uint32_t step) {
   auto qb = [&](uint32_t p) -> uint8_t { return strand ? comp[raw[L - 1 - p]] : upper_dev(raw[p]); };
@@ -182,13 +182,25 @@ __device__ __forceinline__ uint32_t walk_record(const DevIndex& ix, const uint8_
   uint32_t tail = 0;
   if (lq < L && lr < rlen) {
     const uint32_t lim = min(min(rlen - lr, k), L - lq);
-    tail = first_mismatch([&](uint32_t i) { return qb(lq + i); }, [&](uint32_t i) { return rs[lr + i]; }, lim);
+    while (tail + 4 <= lim) {
+      uint32_t wq;
+      if (strand) {
+        const uint32_t w = load4(raw + (L - 4 - (lq + tail)));
+        wq = (uint32_t)comp[w >> 24] | ((uint32_t)comp[(w >> 16) & 0xFFu] << 8) |
+             ((uint32_t)comp[(w >> 8) & 0xFFu] << 16) | ((uint32_t)comp[w & 0xFFu] << 24);
+      } else {
+        wq = upper4(load4(raw + lq + tail));
+      }
+      if (wq ^ load4(rs + lr + tail)) break;
+      tail += 4;
+    }
+    while (tail < lim && qb(lq + tail) == rs[lr + tail]) tail++;
   }
   uint32_t head = 0;
   const uint32_t hsz = min(sr, k);
   if (sq != 0 && hsz != 0) {
     const uint32_t jb = min(sq - 1, hsz - 1);
-    head = first_mismatch([&](uint32_t j) { return qb(sq - 1 - j); }, [&](uint32_t j) { return rs[sr - j]; }, jb);
+    while (head < jb && qb(sq - 1 - head) == rs[sr - head]) head++;
   }
   const uint32_t tot = tail + head + (lq - sq);
   return tot >= k ? ((sq - head) << 16) | tot : 0u;
