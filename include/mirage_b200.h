@@ -176,6 +176,11 @@ int mg_get_tuning(const mg_index* ix, mg_tuning* t, char* density_class, uint64_
  * the buffer itself. */
 int mg_gather_bandwidth(int device, uint64_t buffer_bytes, double* gbs);
 int mg_last_kernel_times(mg_index* ix, float* ms5);
+/* Diagnostic: how many reads each tier of the last batched call run in one piece (the device
+ * form, or host buffers too few to chunk) handed on: [the 64-, 128- and 256-posting dual-strand
+ * tiers, the general warp tier, the smaller and the larger long-read size, the block tier] (the
+ * last goes to the global-memory tier). With first_tier 2 or 3 the tiers before it count 0. */
+int mg_last_tier_counts(mg_index* ix, uint32_t* counts7);
 int mg_bucket_sizes(mg_index* ix, const uint32_t* hashes, uint32_t* counts, uint64_t n);
 
 /* Replaces Hashmap::BuildHashmapTable + SaveHashmapTableV3 (Hashmap.cpp:967, :1701): builds a

@@ -24,7 +24,7 @@ ERRORS = {-1: "MG_ERR_IO", -2: "MG_ERR_BADFMT", -3: "MG_ERR_OOM", -4: "MG_ERR_LI
           -6: "MG_ERR_BADINPUT", -7: "MG_ERR_TIMEOUT", -8: "MG_ERR_INVAL", -9: "MG_ERR_BUSY"}
 
 EXPORTS = ["mg_open", "mg_open_image", "mg_close", "mg_index_get_info", "mg_inspect_image", "mg_eval_logf",
-           "mg_set_timing", "mg_set_probe_slots", "mg_set_tuning", "mg_get_tuning", "mg_last_kernel_times", "mg_bucket_sizes", "mg_gather_bandwidth",
+           "mg_set_timing", "mg_set_probe_slots", "mg_set_tuning", "mg_get_tuning", "mg_last_kernel_times", "mg_last_tier_counts", "mg_bucket_sizes", "mg_gather_bandwidth",
            "mg_build_image", "mg_build_image_device", "mg_parse_fasta_device", "mg_seqs_free", "mg_free",
            "mg_score_batch", "mg_classify", "mg_classify_device", "mg_classify_device_sync",
            "mg_score_candidates", "mg_score_candidates_noalloc", "mg_server_create", "mg_server_submit", "mg_server_submit_into", "mg_server_register_host",
@@ -123,6 +123,7 @@ def lib() -> C.CDLL:
         L.mg_get_tuning.argtypes = [vp, C.POINTER(_Tuning), C.c_char_p, u64]
         L.mg_gather_bandwidth.argtypes = [i32, u64, C.POINTER(C.c_double)]
         L.mg_last_kernel_times.argtypes = [vp, vp]
+        L.mg_last_tier_counts.argtypes = [vp, vp]
         L.mg_bucket_sizes.argtypes = [vp, vp, vp, u64]
         L.mg_inspect_image.argtypes = [vp, u64, i32, C.POINTER(_Info)]
         L.mg_eval_logf.argtypes = [vp, vp, vp, u64]
@@ -337,6 +338,13 @@ class Index:
         ms = np.zeros(5, np.float32)
         _check(lib().mg_last_kernel_times(self.h, ms.ctypes.data), "mg_last_kernel_times")
         return ms
+
+    def last_tier_counts(self) -> dict:
+        """Reads each tier of the last one-piece batched call handed on (mg_last_tier_counts)."""
+        c = np.zeros(7, np.uint32)
+        _check(lib().mg_last_tier_counts(self.h, c.ctypes.data), "mg_last_tier_counts")
+        names = ["dual64", "dual128", "dual256", "warp", "long_small", "long_large", "block"]
+        return {n: int(v) for n, v in zip(names, c)}
 
     def bucket_sizes(self, hashes) -> np.ndarray:
         h = np.ascontiguousarray(hashes, dtype=np.uint32)

@@ -1692,6 +1692,21 @@ int mg_last_kernel_times(mg_index* ix, float* ms) {
   return MG_OK;
 }
 
+int mg_last_tier_counts(mg_index* ix, uint32_t* counts7) {
+  if (!ix || !counts7) return set_error(MG_ERR_INVAL, "null argument");
+  std::lock_guard<std::mutex> lk(ix->mu);
+  CU(cudaSetDevice(ix->device));
+  if (!ix->ws.ctr.p) return set_error(MG_ERR_INVAL, "no batched call yet");
+  uint8_t h[128];
+  CU(cudaStreamSynchronize(ix->stream));
+  CU(cudaMemcpy(h, ix->ws.ctr.p, sizeof(h), cudaMemcpyDeviceToHost));
+  // the lists' counters (run_pipeline): left by the 64-, 128- and 256-posting dual tiers, the
+  // general warp tier, the two long-read sizes and the block tier
+  static const int at[7] = {48, 72, 56, 24, 80, 64, 32};
+  for (int i = 0; i < 7; i++) std::memcpy(&counts7[i], h + at[i], 4);
+  return MG_OK;
+}
+
 __global__ void k_bucket_sizes(const uint32_t* dir, const uint32_t* h, uint32_t* out, uint64_t n) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {

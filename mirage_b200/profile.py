@@ -54,6 +54,7 @@ def main() -> None:
     d_cands = torch.empty(cap * 16, dtype=torch.uint8, device=dev)
     d_nc = torch.zeros(1, dtype=torch.int64, device=dev)
     st = torch.cuda.Stream(device=dev)
+    ix.set_timing(True)
     ms = []
     for _ in range(args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -72,8 +73,11 @@ def main() -> None:
         e1.record(st)
         torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1))
+    extra = {}
+    if args.form == "batched":  # the last step's tier times and the reads each tier handed on
+        extra = {"kernel_ms": [round(float(x), 4) for x in ix.last_kernel_times()], "handed_on": ix.last_tier_counts()}
     print(json.dumps({"workload": args.workload, "scale": args.scale, "reads": n, "bases": int(reads.offs[-1]),
-                      "form": args.form, "index": ix.info(), "shapes": ix.get_tuning()[0], "step_ms": ms}))
+                      "form": args.form, "index": ix.info(), "shapes": ix.get_tuning()[0], "step_ms": ms, **extra}))
     ix.close()
 
 
