@@ -410,3 +410,21 @@ def test_long_reads_past_the_smaller_long_size(tmp_path):
     seqs += [core[20000:20000 + 8192].tobytes(), core[21000:21000 + 8193].tobytes(), core[20500:20500 + 8191].tobytes()]
     r = check_against_oracle(gix, oix, seqs)
     assert (r.reads["n_fwd"][:3] >= 1).all()
+
+
+def test_tier_counts_follow_the_reads(golden):
+    """mg_last_tier_counts after a one-piece batched call: reads of 1-20 kb pass every dual-strand
+    tier and the general warp tier on to the long-read tier (each count at most the batch), and
+    a batch of short reads from the plain references leaves the long-read sizes nothing."""
+    g = golden("long_small")
+    ix = M.Index(g.image)
+    long_reads = g.reads.lengths() > 320
+    ix.classify(g.reads.data, g.reads.offs)
+    c = ix.last_tier_counts()
+    n = len(g.reads)
+    assert all(0 <= v <= n for v in c.values()), c
+    assert c["warp"] >= int(long_reads.sum()) > 0, c
+    gp, (pix, _) = plain_index(golden)
+    pix.classify(gp.reads.data, gp.reads.offs)
+    cp = pix.last_tier_counts()
+    assert cp["long_small"] == 0 and cp["long_large"] == 0 and cp["block"] == 0, cp
