@@ -235,7 +235,32 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
     if (run_from(i) >= keep_min && !lg_contains(S.rt, kLgRT - 1, S.p_ref[i], err))
       if (atomicAdd(&S.n_rt, 1u) < (uint32_t)kLgRT / 2) lg_insert(S.rt, kLgRT - 1, S.p_ref[i], err);
   __syncthreads();
-  if (S.n_rt > (uint32_t)kLgRT / 2) return kStrandOverflow;
+  if (S.n_rt > (uint32_t)kLgRT / 2) {
+    if (keep_min != 1) return kStrandOverflow;
+    // hs = 2 keeps every reference with a posting (max(1, hs - 1) = 1), more than the table
+    // holds. A diagonal run of 2 needs two postings of one reference on one diagonal at
+    // consecutive seeds ((ref, pos, q) then (ref, pos + step, q + step), Analyser.cpp:2337-2402):
+    // when the strand has no such pair its longest run M is below 2 and it has no candidate. The
+    // pairs are looked for through the hash set, now free, of the postings' (ref, diagonal, seed)
+    // keys folded to 32 bits; a collision can only report a pair that is not there, which sends
+    // the strand on as before.
+    auto dkey = [&](uint32_t i, uint32_t dj) -> uint32_t {
+      const uint32_t j = (S.p_fj[i] >> 11) & 0x7FFu;
+      const uint32_t d = S.p_pos[i] - j * step;  // the diagonal, modulo 2^32
+      const uint64_t x = (uint64_t)S.p_ref[i] * 0x9E3779B97F4A7C15ull ^ (uint64_t)d * 0xC2B2AE3D27D4EB4Full ^
+                         (uint64_t)(j + dj) * 0x165667B19E3779F9ull;
+      const uint32_t v = (uint32_t)(x >> 32) ^ (uint32_t)x;
+      return v == kLgEmpty ? kLgEmpty - 1u : v;
+    };
+    for (uint32_t i = tid; i < hsz; i += G) S.hs[i] = kLgEmpty;
+    __syncthreads();
+    for (uint32_t i = tid; i < ne; i += G) lg_insert(S.hs, mask, dkey(i, 0), err);
+    __syncthreads();
+    int pair = 0;
+    for (uint32_t i = tid; i < ne && !pair; i += G) pair = lg_contains(S.hs, mask, dkey(i, 1), err) ? 1 : 0;
+    if (__syncthreads_or(pair)) return kStrandOverflow;
+    return kStrandOk;  // no diagonal run of 2: no candidate on this strand
+  }
   // 3. the kept references' postings, as (refID << 32 | position, query position) sort keys
   uint64_t* kA = reinterpret_cast<uint64_t*>(S.hs);
   constexpr int kK = SM::kK;

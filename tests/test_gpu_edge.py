@@ -428,3 +428,39 @@ def test_tier_counts_follow_the_reads(golden):
     pix.classify(gp.reads.data, gp.reads.offs)
     cp = pix.last_tier_counts()
     assert cp["long_small"] == 0 and cp["long_large"] == 0 and cp["block"] == 0, cp
+
+
+def test_strands_that_keep_every_reference(tmp_path):
+    """A strand whose longest occurrence run is 2 keeps every reference with a posting
+    (max(1, hs - 1) = 1): here about 100, more than the long-read tier's table. Two 1,500-base
+    reads have their seed windows planted one per reference, seeds 0 and 1 both in reference 0.
+    In the first those two lie on different diagonals: no diagonal run of 2 anywhere, so the
+    strand has no candidate and the long-read tier finishes the read itself. In the second they
+    lie on one diagonal: the read goes on to the block tier, which scores reference 0. Both equal
+    the oracle, and the tier counts show the two paths."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(61)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    k, step, hlen, L = 31, 15, 17, 1500
+    ns = (L - k + step - 1) // step
+    reads = [acgt[rng.integers(0, 4, L)] for _ in range(2)]
+    refs = [acgt[rng.integers(0, 4, 5000)].copy() for _ in range(2 * ns + 2)]
+    r0 = refs[0]
+    a, b = reads
+    r0[100:100 + hlen] = a[0:hlen]                 # seed 0 of the first read ...
+    r0[2000:2000 + hlen] = a[step:step + hlen]     # ... and seed 1, on another diagonal
+    r0[3000:3000 + step + hlen] = b[0:step + hlen]  # seeds 0 and 1 of the second read, one diagonal
+    for j in range(2, ns):
+        refs[j][500:500 + hlen] = a[j * step:j * step + hlen]
+        refs[ns + j][700:700 + hlen] = b[j * step:j * step + hlen]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))], k=k)
+    path = tmp_path / "keepall.mhm"
+    image.tofile(path)
+    gix, oix = M.Index(image, k=k), O.Index(str(path), k=k)
+    r = check_against_oracle(gix, oix, [a.tobytes(), b.tobytes()])
+    c = gix.last_tier_counts()
+    assert c["warp"] == 2 and c["long_small"] == 1 and c["long_large"] == 1, c
+    assert r.reads["n_fwd"][0] == 0 and r.reads["n_fwd"][1] >= 1
