@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1363,7 +1364,7 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   const uint64_t pack_need = n_bases / 4 + 64 * (uint64_t)(nc + 1), exc_need = n_bases / 32 + 4096 * (uint64_t)nc;
   if (pack) {
     if (!ix->pack_pool)
-      ix->pack_pool = new PackPool(pack_threads());
+      ix->pack_pool = new PackPool(std::max(1, pack_threads() - 1));  // a CPU left for the launches
     if (ix->h_pack_cap < pack_need) {
       if (ix->h_pack) cudaFreeHost(ix->h_pack);
       ix->h_pack = nullptr;
@@ -1380,7 +1381,42 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
     }
     if (w.packed.alloc(pack_need) || w.exc.alloc(exc_need * 8)) return set_error(MG_ERR_OOM, "packed staging");
   }
-  uint64_t pk = 0, ek = 0;  // staging offsets of the next chunk's packed bytes and exceptions
+  // the packed upload: a packer thread packs the chunks in order, ahead of this thread, which
+  // enqueues each chunk's copies and kernels once its bytes are packed; each chunk has its own
+  // staging region and an equal share of the exception staging (a chunk with more exceptions
+  // goes up as given)
+  uint64_t pk_at[mg_index::kMaxChunks + 1] = {0};
+  const uint64_t exc_share = exc_need / (uint64_t)std::max(1, nc);
+  for (int i = 0; i < nc; i++) {
+    const uint64_t nb_i = batch->offsets[bound[i + 1]] - batch->offsets[bound[i]];
+    pk_at[i + 1] = pk_at[i] + ((nb_i + 3) / 4 + 15) / 16 * 16;
+  }
+  struct Packer {
+    std::mutex mu;
+    std::condition_variable cv;
+    int64_t n_exc[mg_index::kMaxChunks];  // per chunk: exceptions, -1 not packed yet, -2 too many
+    std::atomic<bool> stop{false};
+    std::thread th;
+    ~Packer() {  // joined on every way out of the call
+      stop = true;
+      if (th.joinable()) th.join();
+    }
+  } packer;
+  for (int i = 0; i < mg_index::kMaxChunks; i++) packer.n_exc[i] = -1;
+  if (pack) {
+    packer.th = std::thread([&] {
+      for (int i = 0; i < nc && !packer.stop; i++) {
+        const uint64_t b0 = batch->offsets[bound[i]], b1 = batch->offsets[bound[i + 1]];
+        uint64_t ne = 0;
+        if (b1 > b0)
+          pack_bases(*ix->pack_pool, batch->bases + b0, b1 - b0, ix->h_pack + pk_at[i], ix->h_exc + i * exc_share,
+                     exc_share, &ne);
+        std::lock_guard<std::mutex> lk(packer.mu);
+        packer.n_exc[i] = ne <= exc_share ? (int64_t)ne : -2;
+        packer.cv.notify_one();
+      }
+    });
+  }
   for (int i = 0; i < nc && rc == MG_OK; i++) {
     const uint64_t r0 = bound[i], r1 = bound[i + 1];
     const uint64_t b0 = batch->offsets[r0], b1 = batch->offsets[r1];
@@ -1390,12 +1426,12 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
                        ix->h2d));
     bool packed = false;
     uint64_t n_exc = 0;
-    const uint64_t pb = (b1 - b0 + 3) / 4;
+    const uint64_t pb = (b1 - b0 + 3) / 4, pk = pk_at[i], ek = (uint64_t)i * exc_share;
     if (pack && b1 > b0) {
-      // packed on the host while the device works on the earlier chunks
-      const uint64_t cap = (exc_need - ek) / (uint64_t)(nc - i);
-      pack_bases(*ix->pack_pool, batch->bases + b0, b1 - b0, ix->h_pack + pk, ix->h_exc + ek, cap, &n_exc);
-      packed = n_exc <= cap;
+      std::unique_lock<std::mutex> lk(packer.mu);
+      packer.cv.wait(lk, [&] { return packer.n_exc[i] != -1; });
+      packed = packer.n_exc[i] >= 0;
+      n_exc = packed ? (uint64_t)packer.n_exc[i] : 0;
     }
     if (packed) {
       CU(cudaMemcpyAsync(w.packed.as<uint8_t>() + pk, ix->h_pack + pk, pb, cudaMemcpyHostToDevice, ix->h2d));
@@ -1414,8 +1450,6 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
         k_unpack_exceptions<<<(unsigned)std::min<uint64_t>((n_exc + 255) / 256, (uint64_t)sms * 4), 256, 0, st>>>(
             w.exc.as<uint64_t>() + ek, n_exc, b1 - b0, w.bases.as<uint8_t>() + b0);
       CU(cudaGetLastError());
-      pk += (pb + 15) / 16 * 16;
-      ek += n_exc;
     }
     const ChainSync cs{i ? ix->ev_scan[i - 1] : nullptr, ix->ev_scan[i], ix->h_snap + i};
     rc = run_pipeline(ix, *cws[i & 1], r1 - r0, w.offs.as<uint64_t>() + r0, w.bases.as<uint8_t>(),
