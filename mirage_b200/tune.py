@@ -39,7 +39,7 @@ SHORT_GRID = {
     "finish_blocks_per_sm": [2, 4, 8],
 }
 LONG_GRID = {"long_blocks_per_sm": [1, 2]}
-E2E_GRID = {"chunks": [4, 6, 8], "weighted_chunks": [1, 2]}
+E2E_GRID = {"chunks": [4, 6, 8], "weighted_chunks": [1, 2], "pack_bases": [1, 2]}
 
 
 def tuning_path(device: int = 0) -> str:
@@ -167,6 +167,7 @@ def tune(ix: M.Index, reads, grid: dict, seconds: float = 60.0, reps: int = 5, e
 
         ix.set_tuning(**best)
         e2e_best = e2e_ms()
+        e2e_want = h_reads.numpy().tobytes()
         out["e2e_trials"] = [{"fields": dict(best), "ms": e2e_best}]
         for field, values in E2E_GRID.items():
             for v in values:
@@ -177,6 +178,8 @@ def tune(ix: M.Index, reads, grid: dict, seconds: float = 60.0, reps: int = 5, e
                     continue
                 ix.set_tuning(**cand)
                 ms = e2e_ms()
+                if h_reads.numpy().tobytes() != e2e_want:
+                    raise RuntimeError(f"launch shapes {cand} changed the results end to end")
                 out["e2e_trials"].append({"fields": cand, "ms": ms})
                 if ms < e2e_best:
                     best, e2e_best = cand, ms
