@@ -1298,6 +1298,13 @@ int error_status(int err) {
 // one piece, and from kMaxChunks times this on the chunks are weighted (1,000,000 reads: 8
 // chunks, the first and last 55,556 reads).
 constexpr uint64_t kChunkReads = 65536;
+constexpr uint64_t kChunkBases = kChunkReads * 192;  // the same size in bases, for long reads
+
+// Chunks of a host-buffer batch: by reads or by bases, whichever gives more (long reads fill a
+// chunk with few of them); 1 or less runs the batch in one piece.
+static uint64_t chunk_units(uint64_t n, uint64_t n_bases) {
+  return std::min<uint64_t>(n, std::max<uint64_t>(n / kChunkReads, n_bases / kChunkBases));
+}
 constexpr int kRunWhole = 1;
 
 // Threads of the packed upload's pool: one per CPU this process may run on, at most 32 (a thread
@@ -1332,7 +1339,7 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   }
   if (w.chain.alloc(16)) return set_error(MG_ERR_OOM, "chunk counters");
   const Shapes sh = shapes(ix);
-  const int nc = (int)std::min<uint64_t>(sh.chunks, n / kChunkReads);
+  const int nc = (int)std::min<uint64_t>(sh.chunks, chunk_units(n, batch->offsets[n]));
   // chunk boundaries, weighted so that the first chunk (whose upload nothing hides) and the last
   // (whose classification and copy back nothing hides) are the smallest
   static const int kWeight[mg_index::kMaxChunks] = {1, 2, 3, 3, 3, 3, 2, 1};
@@ -1503,7 +1510,7 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   if (w.cands.alloc(std::max<uint64_t>(out->cand_cap, 1) * sizeof(mg_candidate)))
     return set_error(MG_ERR_OOM, "candidate buffer");
   bool chunks_overflowed = false;
-  if (!plain && n >= 2 * kChunkReads && shapes(ix).chunks > 1) {
+  if (!plain && chunk_units(n, nb) >= 2 && shapes(ix).chunks > 1) {
     rc = classify_chunked(ix, w, batch, out);
     if (rc != kRunWhole) return rc;
     chunks_overflowed = true;

@@ -464,3 +464,25 @@ def test_strands_that_keep_every_reference(tmp_path):
     c = gix.last_tier_counts()
     assert c["warp"] == 2 and c["long_small"] == 1 and c["long_large"] == 1, c
     assert r.reads["n_fwd"][0] == 0 and r.reads["n_fwd"][1] >= 1
+
+
+def test_long_reads_chunked_by_bases(golden):
+    """A host-buffer batch of few but long reads (over 2 x 12.6 Mbp in all, well under 131,072
+    reads) is split into chunks by its bases, so that the copy of one chunk overlaps the work on
+    the one before; the results equal those of the batch run in one piece, byte for byte."""
+    g = golden("long_small")
+    ix = M.Index(g.image)
+    reps = max(1, int(np.ceil(30e6 / float(g.reads.offs[-1]))))
+    lens = g.reads.lengths()
+    offs = np.zeros(len(lens) * reps + 1, np.uint64)
+    offs[1:] = np.cumsum(np.tile(lens, reps))
+    data = np.tile(g.reads.data[: int(g.reads.offs[-1])], reps)
+    assert offs[-1] > 2 * 65536 * 192 and len(offs) - 1 < 2 * 65536
+    chunked = ix.classify(data, offs)
+    ix.set_tuning(chunks=1)
+    try:
+        whole = ix.classify(data, offs)
+    finally:
+        ix.set_tuning()
+    assert np.array_equal(chunked.reads.view(np.uint8), whole.reads.view(np.uint8))
+    assert np.array_equal(chunked.cands.view(np.uint8), whole.cands.view(np.uint8))
