@@ -217,7 +217,9 @@ def main() -> None:
     fields = res["fields"] if args.workload != "long" else {k: res["fields"][k] for k in LONG_GRID}
     write_tuning_file(path, cls, fields,
                       note=f"{cls}: {args.workload} workload, {len(reads)} reads; device step {res['ms_per_step']:.3f} ms "
-                           f"(defaults {res['default_ms_per_step']:.3f} ms)")
+                           f"(defaults {res['default_ms_per_step']:.3f} ms)"
+                           + (f"; end to end {res['e2e_ms']:.3f} ms (first setting {res['e2e_trials'][0]['ms']:.3f} ms)"
+                              if res.get("e2e_trials") else ""))
     print(json.dumps({"class": cls, "file": path, **{k: v for k, v in res.items() if k != "trials"},
                       "n_trials": len(res["trials"])}))
     ix.close()
