@@ -1216,8 +1216,8 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
       CU(cudaEventRecord(w.fork, st));
       CU(cudaStreamWaitEvent(w.side, w.fork, 0));
       if (tm) CU(cudaEventRecord(ix->ev[2], w.side));
-      int per_sm2 = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
+      static int per_sm2 = 0;  // the same on every call (one architecture): queried once
+      if (!per_sm2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_classify_warp_list, kW1Warps * 32, 0);
       k_classify_warp_list<<<(unsigned)std::max(1, per_sm2) * sms, kW1Warps * 32, 0, w.side>>>(ix->dix, b, sd);
       if (tm) CU(cudaEventRecord(ix->ev[3], w.side));
       k_classify_long<LongSmemS, 4><<<sh.long_small_blocks_per_sm * sms, kLgThreads, sizeof(LongSmemS), w.side>>>(
