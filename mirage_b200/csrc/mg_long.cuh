@@ -52,6 +52,8 @@ struct alignas(16) LongSmemT {
   RedTmp<kLgThreads> red;
   uint32_t n_kept, n_rt;
   uint32_t scored[kLgC / 32];  // candidates with a score (bit per candidate)
+  uint32_t rrank[kLgRT];       // kept reference of a table slot: its rank by refID
+  uint32_t bcnt[kLgRT / 2], bfill[kLgRT / 2], boff[kLgRT / 2 + 1], bmax;  // the kept references' ranges
   uint32_t n_sc;
   float hi;
   uint8_t q[Q];               // strand bases
@@ -75,6 +77,18 @@ __device__ __forceinline__ bool lg_contains(const uint32_t* set, uint32_t mask, 
   }
   *err |= kErrInternal;
   return false;
+}
+
+// The slot holding key, or -1 (bounded like lg_contains).
+__device__ __forceinline__ int lg_find(const uint32_t* set, uint32_t mask, uint32_t key, int* err) {
+  uint32_t s = lg_mix(key) & mask;
+  for (uint32_t n = 0; n <= mask; n++, s = (s + 1) & mask) {
+    const uint32_t v = set[s];
+    if (v == key) return (int)s;
+    if (v == kLgEmpty) return -1;
+  }
+  *err |= kErrInternal;
+  return -1;
 }
 
 // Inserts key; true when this call inserted it (false: it was there already).
@@ -261,30 +275,99 @@ __device__ int long_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, i
     if (__syncthreads_or(pair)) return kStrandOverflow;
     return kStrandOk;  // no diagonal run of 2: no candidate on this strand
   }
-  // 3. the kept references' postings, as (refID << 32 | position, query position) sort keys
+  // 3. the kept references' postings as (refID << 32 | position, query position) sort keys,
+  //    grouped by reference: the kept references (at most kLgRT / 2) ranked by refID, each one's
+  //    postings counted and given a range in that order, then scattered into it
   uint64_t* kA = reinterpret_cast<uint64_t*>(S.hs);
   constexpr int kK = SM::kK;
+  constexpr int kBk = kLgRT / 2;  // ranges
   uint32_t* kB = S.hs + 2 * kK;
-  for (uint32_t i = tid; i < ne; i += G) {
-    const uint32_t ref = S.p_ref[i];
-    if (lg_contains(S.rt, kLgRT - 1, ref, err)) {
-      const uint32_t t = atomicAdd(&S.n_kept, 1u);
-      if (t < (uint32_t)kK) {
-        kA[t] = ((uint64_t)ref << 32) | S.p_pos[i];
-        kB[t] = ((S.p_fj[i] >> 11) & 0x7FFu) * step;
+  if (tid < kLgRT) {
+    const uint32_t r = S.rt[tid];
+    uint32_t rk = 0;
+    if (r != kLgEmpty)
+      for (int s2 = 0; s2 < kLgRT; s2++) {
+        const uint32_t r2 = S.rt[s2];
+        rk += (r2 != kLgEmpty && r2 < r) ? 1u : 0u;
       }
+    S.rrank[tid] = rk;
+  }
+  if (tid < kBk) {
+    S.bcnt[tid] = 0;
+    S.bfill[tid] = 0;
+  }
+  __syncthreads();
+  for (uint32_t i = tid; i < ne; i += G) {
+    const int sl = lg_find(S.rt, kLgRT - 1, S.p_ref[i], err);
+    if (sl >= 0) atomicAdd(&S.bcnt[S.rrank[sl]], 1u);
+  }
+  __syncthreads();
+  if (tid < 32) {  // the ranges' starts (two per lane), their total and the largest range
+    const unsigned FULL = 0xFFFFFFFFu;
+    const uint32_t c0 = S.bcnt[2 * tid], c1 = S.bcnt[2 * tid + 1];
+    uint32_t x = c0 + c1;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, x, o);
+      if (tid >= o) x += y;
     }
+    const uint32_t ex = x - (c0 + c1);
+    S.boff[2 * tid] = ex;
+    S.boff[2 * tid + 1] = ex + c0;
+    if (tid == 31) {
+      S.boff[kBk] = x;
+      S.n_kept = x;
+    }
+    const uint32_t mb = __reduce_max_sync(FULL, max(c0, c1));
+    if (tid == 0) S.bmax = mb;
   }
   __syncthreads();
   const int T2 = (int)S.n_kept;
   if (T2 > kK) return kStrandOverflow;
-  const int N = next_pow2(T2);
-  for (int i = T2 + tid; i < N; i += G) {
-    kA[i] = ~0ull;
-    kB[i] = ~0u;
+  for (uint32_t i = tid; i < ne; i += G) {
+    const int sl = lg_find(S.rt, kLgRT - 1, S.p_ref[i], err);
+    if (sl >= 0) {
+      const uint32_t b = S.rrank[sl];
+      const uint32_t t = S.boff[b] + atomicAdd(&S.bfill[b], 1u);
+      kA[t] = ((uint64_t)S.p_ref[i] << 32) | S.p_pos[i];
+      kB[t] = ((S.p_fj[i] >> 11) & 0x7FFu) * step;
+    }
   }
   __syncthreads();
-  bitonic_sort<G>(kA, kB, N);
+  if (S.bmax <= 128u) {
+    // each range sorted by (position, query position), a warp per range: an entry's place is the
+    // number of its range's entries with a smaller key (the keys are distinct), written to the
+    // postings' arrays, free by now, and copied back
+    const uint32_t lane = (uint32_t)tid & 31u, warp = (uint32_t)tid >> 5;
+    for (uint32_t b = warp; b < (uint32_t)kBk; b += G / 32) {
+      const uint32_t b0 = S.boff[b], b1 = S.boff[b + 1];
+      for (uint32_t e = b0 + lane; e < b1; e += 32) {
+        const uint64_t ka = kA[e];
+        const uint32_t kb = kB[e];
+        uint32_t rk = 0;
+        for (uint32_t f = b0; f < b1; f++) {
+          const uint64_t fa = kA[f];
+          rk += (fa < ka || (fa == ka && kB[f] < kb)) ? 1u : 0u;
+        }
+        S.p_ref[b0 + rk] = (uint32_t)(ka >> 32);
+        S.p_pos[b0 + rk] = (uint32_t)ka;
+        S.p_fj[b0 + rk] = kb;
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < T2; i += G) {
+      kA[i] = ((uint64_t)S.p_ref[i] << 32) | S.p_pos[i];
+      kB[i] = S.p_fj[i];
+    }
+    __syncthreads();
+  } else {  // a large range (a read from one reference): one bitonic sort of all the keys
+    const int N = next_pow2(T2);
+    for (int i = T2 + tid; i < N; i += G) {
+      kA[i] = ~0ull;
+      kB[i] = ~0u;
+    }
+    __syncthreads();
+    bitonic_sort<G>(kA, kB, N);
+  }
   // 4. diagonal runs (Analyser.cpp:2337-2490): X = position within the run, Y = longest run of
   //    the reference
   uint32_t* X = S.p_ref;
