@@ -78,7 +78,7 @@ typedef struct {
 } mg_read_result;
 
 #define MG_READ_BAD_BYTE 0xFF   /* the read holds a byte without a reverse complement */
-#define MG_READ_TOO_LARGE 0xFE  /* the read exceeds the largest workspace tier */
+#define MG_READ_TOO_LARGE 0xFE  /* the read exceeds the oversize tier's limits */
 
 /* One scored candidate (a MatrixResult::ResultsScores entry with its raw score). Candidates
  * of a strand are in ascending refID order, as CreateResultsScores emits them. */
@@ -212,12 +212,18 @@ int mg_build_image_device(int device, const uint8_t* bases, const uint64_t* offs
 /* Plain form. Replaces the reference's per-batch sequence TPrepareGPUAnalysis (Analyser.cpp:
  * 1317) -> CPUGetHighestScore (MatrixCPU.cpp:417) -> strand merge (Analyser.cpp:592-611):
  * one block per read in one launch per batch (the global-memory tier takes reads beyond its
- * shared memory), host buffers in and out with synchronous copies. */
+ * shared memory), host buffers in and out with synchronous copies.
+ * Read lengths: like the reference's CPU path, no cap below 2,000,000 bases (the batched forms
+ * too; the served form takes up to 65,535). Reads past 65,535 bases, 4,400 seeds or 65,536
+ * postings per strand go to the oversize tier, whose device workspace is sized by the first
+ * batch that needs it: that batch runs a second time once it has grown (up to 1 GiB, a strand
+ * of at most 2^24 postings); a read beyond those limits fails the call with MG_ERR_LIMIT and is
+ * marked MG_READ_TOO_LARGE. */
 int mg_score_batch(mg_index* ix, const mg_batch* batch, mg_result* out);
 
-/* Batched form: the same results from the fused persistent kernel (warp per read with work
- * stealing, block tier for oversized reads), pipelined copies on streams and a captured CUDA
- * graph. Host buffers in and out. */
+/* Batched form: the same results from the tiered persistent kernels (a warp per read with work
+ * stealing first, larger tiers for the reads it hands on), copies of one chunk overlapped with
+ * the classification of the one before on streams. Host buffers in and out. */
 int mg_classify(mg_index* ix, const mg_batch* batch, mg_result* out);
 
 /* Batched form on device-resident buffers (no host copies): d_offsets / d_bases / outputs are

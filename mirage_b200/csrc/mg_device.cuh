@@ -47,6 +47,7 @@ enum : int {
   kErrLogRange = 8,   // relative-score log outside the patched domain
   kErrArena = 16,     // staging arena too small for the reads with more than kSlots candidates
   kErrInternal = 32,  // a bounded device loop reached its bound (an invariant failed)
+  kErrHuge = 64,      // a read needs a larger oversize-tier workspace (the host grows it and reruns)
 };
 
 struct BatchDev {

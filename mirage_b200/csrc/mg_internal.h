@@ -41,13 +41,24 @@ struct DevBuf {
 struct Workspace {
   DevBuf offs, bases, reads, stage, arena, cands, ctr, ovf, sums, gws, chain;
   DevBuf packed, exc;  // 2-bit packed bases and their exceptions (mg_classify with pack_bases)
+  // the oversize tier: off (hmode 0: the global tier marks what it cannot take) until a batch on
+  // this workspace needs it; its workspace, hslabs slabs, each for a read of up to hq bases,
+  // hseeds seeds and he postings per strand (a power of two) with up to hc candidates per strand,
+  // grown on demand by complete_pipeline
+  DevBuf hws;
+  int hmode = 0;
+  int hslabs = 0;
+  uint32_t hq = 0, hseeds = 0, he = 0, hc = 0;
   // the stream on which the tiers after the dual tier run beside its finishing pass, and the
   // events that fork it from and join it back to the call's stream (made at first use)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   void release() {
-    for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws, &chain, &packed, &exc})
+    for (DevBuf* b : {&offs, &bases, &reads, &stage, &arena, &cands, &ctr, &ovf, &sums, &gws, &chain, &packed, &exc,
+                      &hws})
       b->release();
+    hmode = hslabs = 0;
+    hq = hseeds = he = hc = 0;
     if (side) cudaStreamDestroy(side);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
@@ -56,7 +67,7 @@ struct Workspace {
   }
   size_t bytes() const {
     return offs.n + bases.n + reads.n + stage.n + arena.n + cands.n + ctr.n + ovf.n + sums.n + gws.n + chain.n +
-           packed.n + exc.n;
+           packed.n + exc.n + hws.n;
   }
 };
 
@@ -84,11 +95,14 @@ struct Counters {
   uint64_t n_cands = 0;     // candidates of the batch (written when they fit the output)
   uint64_t arena_need = 0;  // staging arena entries the batch asked for
   int err = 0;              // error bits
-  bool reran = false;       // the batch ran again with a larger staging arena
+  bool reran = false;       // the batch ran again with a larger staging arena or oversize workspace
+  uint32_t huge_need[4] = {0, 0, 0, 0};  // oversize reads that did not fit: most bases, seeds,
+                                         // postings per strand; how many
 };
 int read_counters(Workspace& ws, cudaStream_t st, Counters* c);
-// Waits for a launched pipeline and, when the staging arena was too small, grows it to what the
-// kernels asked for and runs the batch again (same arguments as the launch).
+// Waits for a launched pipeline and, when the staging arena or the oversize tier's workspace was
+// too small, grows it to what the kernels asked for and runs the batch again (same arguments as
+// the launch), up to three times.
 int complete_pipeline(mg_index* ix, Workspace& ws, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                       mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain,
                       Counters* c);

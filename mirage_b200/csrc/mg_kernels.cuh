@@ -39,6 +39,8 @@ struct StrandWS {
   uint32_t* X;         // per-entry scratch
   uint32_t* Y;         // per-entry scratch
   mg_candidate* cb[2]; // scored candidates of the forward and reverse strands
+  uint32_t* W;         // wide form only: per-entry covered-interval start
+  uint32_t* cov;       // wide form only: coverage bitmap of one candidate, (q + 31) / 32 words
 };
 
 enum StrandStatus { kStrandOk = 0, kStrandOverflow = 1, kStrandBad = 2 };
@@ -107,7 +109,12 @@ __device__ __forceinline__ uint32_t tail_walk(const uint8_t* q, const uint8_t* r
 // One strand. Returns kStrandOverflow when the read does not fit the workspace caps (the
 // caller hands the read to a larger tier); on success *n_out scored candidates are in cb and
 // *highest is the strand's HighestScore.
-template <int G>
+// Wide (the oversize tier): found indexes, posting indexes and query positions need not fit 16
+// bits. The occurrence sort then keys (refID << 32 | found index) with the posting index as the
+// secondary key, a run's covered interval keeps its start in ws.W and its length in ws.X, and a
+// candidate's coverage is OR-ed into the bitmap ws.cov; the order of every sort and the values
+// compared are the same as in the packed form.
+template <int G, bool Wide = false>
 __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L, int strand,
                               const StrandWS& ws, const Caps& caps, RedTmp<G>* red, int* err,
                               uint32_t* n_out, float* highest) {
@@ -155,7 +162,12 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
       for (uint32_t t = 0; t < cnt; t++) {
         const uint2 p = __ldg(ix.post + o0 + t);
         ws.X[e + t] = p.y;
-        ws.kA[e + t] = ((uint64_t)p.x << 32) | ((uint64_t)f << 16) | (uint64_t)(e + t);
+        if (Wide) {
+          ws.kA[e + t] = ((uint64_t)p.x << 32) | (uint64_t)f;
+          ws.kB[e + t] = e + t;
+        } else {
+          ws.kA[e + t] = ((uint64_t)p.x << 32) | ((uint64_t)f << 16) | (uint64_t)(e + t);
+        }
       }
     }
     nf += fr;
@@ -165,13 +177,16 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
   if (ne == 0) return kStrandOk;  // nothing to filter: the reference skips the read
   const int T = (int)ne;
   const int N = next_pow2(T);
-  for (int i = T + tid; i < N; i += G) ws.kA[i] = ~0ull;
+  for (int i = T + tid; i < N; i += G) {
+    ws.kA[i] = ~0ull;
+    if (Wide) ws.kB[i] = ~0u;
+  }
   Grp<G>::sync();
   // 2. occurrence filter over (refID, found index)
-  bitonic_sort<G>(ws.kA, nullptr, N);
+  bitonic_sort<G>(ws.kA, Wide ? ws.kB : nullptr, N);
   uint64_t* kA = ws.kA;
   auto refA = [&](int i) { return (uint32_t)(kA[i] >> 32); };
-  auto fA = [&](int i) { return (uint32_t)((kA[i] >> 16) & 0xFFFFu); };
+  auto fA = [&](int i) { return Wide ? (uint32_t)kA[i] : (uint32_t)((kA[i] >> 16) & 0xFFFFu); };
   auto obrk = [&](int i) { return i == 0 || refA(i) != refA(i - 1) || fA(i) > fA(i - 1) + 1; };
   arr_seg_scan<G, false>(ws.Y, T,
                          [&](int i) -> uint32_t { return obrk(i) ? 1u : (fA(i) == fA(i - 1) + 1 ? 1u : 0u); },
@@ -196,7 +211,8 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
     for (int i = tid * C; i < T && i < (tid + 1) * C; i++) {
       const uint64_t key = kA[i];
       if (ws.Y[i] >= keep_min) {
-        const uint32_t idx = (uint32_t)(key & 0xFFFFu), f = (uint32_t)((key >> 16) & 0xFFFFu);
+        const uint32_t idx = Wide ? ws.kB[i] : (uint32_t)(key & 0xFFFFu);
+        const uint32_t f = Wide ? (uint32_t)key : (uint32_t)((key >> 16) & 0xFFFFu);
         kA[i] = ((key >> 32) << 32) | (uint64_t)ws.X[idx];
         ws.kB[i] = ws.fpos[f];
         kept++;
@@ -248,7 +264,14 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
         const uint32_t tail = tail_walk(ws.q, rs, L, rlen, lq, lr, k);
         const uint32_t head = head_walk(ws.q, rs, sq, sr, k);
         const uint32_t tot = tail + head + (lq - sq);
-        if (tot >= k) z = ((sq - head) << 16) | tot;
+        if (Wide) {
+          if (tot >= k) {
+            z = tot;
+            ws.W[i] = sq - head;
+          }
+        } else if (tot >= k) {
+          z = ((sq - head) << 16) | tot;
+        }
       }
       X[i] = z;
     }
@@ -285,7 +308,7 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
     for (int i = sa + tid; i < sb; i += G) {
       const uint32_t z = X[i];
       if (z) {
-        const uint64_t t = z & 0xFFFFu;
+        const uint64_t t = Wide ? z : z & 0xFFFFu;
         sc += t;
         sr += (t * (t + 1)) / 2;
       }
@@ -294,7 +317,25 @@ __device__ int process_strand(const DevIndex& ix, const uint8_t* raw, uint32_t L
     sr = grp_sum_u64<G>(sr, red);
     if (sc == 0) continue;  // Score stays -2
     uint32_t hits = 0;
-    for (uint32_t w = tid; w < nw; w += G) {
+    if (Wide) {
+      // covered intervals OR-ed into the bitmap: work in proportion to the intervals' lengths,
+      // not to (read words x run records)
+      for (uint32_t w = tid; w < nw; w += G) ws.cov[w] = 0;
+      Grp<G>::sync();
+      for (int i = sa + tid; i < sb; i += G) {
+        const uint32_t t = X[i];
+        if (!t) continue;
+        const uint32_t a = ws.W[i], b = a + t;  // b <= L: the tail walk stops at the read's end
+        for (uint32_t w = a >> 5; w <= (b - 1) >> 5; w++) {
+          const uint32_t w0 = w * 32, lo = a > w0 ? a : w0, up = b < w0 + 32 ? b : w0 + 32;
+          const uint32_t n = up - lo;
+          atomicOr(ws.cov + w, (n == 32 ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (lo - w0));
+        }
+      }
+      Grp<G>::sync();
+      for (uint32_t w = tid; w < nw; w += G) hits += __popc(ws.cov[w]);
+    }
+    for (uint32_t w = tid; !Wide && w < nw; w += G) {
       uint32_t bits = 0;
       const uint32_t w0 = w * 32, w1 = w0 + 32;
       for (int i = sa; i < sb; i++) {
@@ -376,22 +417,22 @@ __device__ __forceinline__ void write_read_result(const BatchDev& b, uint32_t r,
 
 // Both strands of read r, the strand merge and the staging write. Returns false when the
 // read must go to a larger tier.
-template <int G>
+template <int G, bool Wide = false>
 __device__ bool process_read(const DevIndex& ix, const BatchDev& b, uint32_t r, const StrandWS& ws,
                              const Caps& caps, RedTmp<G>* red, mg_candidate* stage, mg_candidate* arena,
                              uint64_t arena_cap, unsigned long long* arena_n, int* errw) {
   const int tid = Grp<G>::tid();
   const uint64_t o0 = b.offs[r];
   const uint64_t Lr = b.offs[r + 1] - o0;
-  if (Lr > 0xFFFFu) return false;
+  if (Lr > (Wide ? (uint64_t)caps.q : 0xFFFFull)) return false;
   const uint32_t L = (uint32_t)Lr;
   const uint8_t* raw = b.bases + o0;
   int err = 0;
   uint32_t n[2] = {0, 0};
   float h[2] = {-1.0f, -1.0f};
-  int st = process_strand<G>(ix, raw, L, 0, ws, caps, red, &err, &n[0], &h[0]);
+  int st = process_strand<G, Wide>(ix, raw, L, 0, ws, caps, red, &err, &n[0], &h[0]);
   if (st == kStrandOverflow) return false;
-  if (st != kStrandBad) st = process_strand<G>(ix, raw, L, 1, ws, caps, red, &err, &n[1], &h[1]);
+  if (st != kStrandBad) st = process_strand<G, Wide>(ix, raw, L, 1, ws, caps, red, &err, &n[1], &h[1]);
   if (st == kStrandOverflow) return false;
   if (tid == 0) write_read_result(b, r, st == kStrandBad, n, h, ws.cb, stage, arena, arena_cap, arena_n, errw, err);
   Grp<G>::sync();

@@ -74,12 +74,21 @@ constexpr int kB2Q = 20480, kB2Seeds = 1408, kB2E = 4096, kB2C = 128;
 constexpr int kB3Threads = 256;
 constexpr int kB3Q = 65535, kB3Seeds = 4400, kB3E = 65536, kB3C = 4096;
 constexpr int kB3Blocks = 32;
+// Oversize tier: what the global tier cannot hold (reads over 65,535 bases, or over 4,400 seeds
+// or 65,536 postings per strand), one block per read over a workspace sized on demand for the
+// largest such read, 32-bit fields throughout. Hard limits: a read of at most 2,000,000 bases
+// (the relative score's logarithm stays inside its patched domain up to there) and 2^24
+// postings per strand; at most 4 workspaces and 1 GiB.
+constexpr int kHugeThreads = 512;
+constexpr uint32_t kHugeMaxQ = 2000000, kHugeMaxE = 1u << 24;
+constexpr int kHugeMaxSlabs = 4;
+constexpr size_t kHugeMaxBytes = size_t(1) << 30;
 
 struct WsLayout {
-  size_t kA, kB, X, Y, fpos, cb, q, red, total;
+  size_t kA, kB, X, Y, fpos, cb, q, red, W, cov, total;
 };
 
-static WsLayout ws_layout(int Q, int seeds, int E, int C) {
+static WsLayout ws_layout(int Q, int seeds, int E, int C, bool wide = false) {
   WsLayout l;
   size_t o = 0;
   auto take = [&](size_t n, size_t al) {
@@ -96,6 +105,8 @@ static WsLayout ws_layout(int Q, int seeds, int E, int C) {
   l.cb = take((size_t)2 * C * sizeof(mg_candidate), 16);
   l.q = take((size_t)Q, 16);
   l.red = take(sizeof(RedTmp<256>), 16);
+  l.W = wide ? take((size_t)E * 4, 16) : 0;
+  l.cov = wide ? take(((size_t)Q + 31) / 32 * 4, 16) : 0;
   l.total = (o + 127) / 128 * 128;
   return l;
 }
@@ -110,6 +121,8 @@ __device__ __forceinline__ StrandWS ws_from(uint8_t* base, const WsLayout& l, in
   ws.cb[0] = (mg_candidate*)(base + l.cb);
   ws.cb[1] = ws.cb[0] + C;
   ws.q = base + l.q;
+  ws.W = l.W ? (uint32_t*)(base + l.W) : nullptr;
+  ws.cov = l.cov ? (uint32_t*)(base + l.cov) : nullptr;
   return ws;
 }
 
@@ -427,7 +440,9 @@ __global__ void __launch_bounds__(kLgThreads, MinBlocks) k_classify_long(DevInde
   }
 }
 
-// Block tier over a list of reads (list == nullptr: every read, the plain form).
+// Block tier over a list of reads (list == nullptr: every read, the plain form); the reads that
+// do not fit go to the next list, or, from the last tier, are marked for the oversize tier
+// (kErrHuge: the host then runs the batch again with it).
 template <int G>
 __global__ void __launch_bounds__(G) k_classify_block(DevIndex ix, BatchDev b, StageDev sd, const uint32_t* list,
                                                        const unsigned* list_n, unsigned* cursor, uint32_t* next,
@@ -450,16 +465,89 @@ __global__ void __launch_bounds__(G) k_classify_block(DevIndex ix, BatchDev b, S
     if (!process_read<G>(ix, b, r, ws, caps, red, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err)) {
       if (threadIdx.x == 0) {
         if (last_tier) {
-          atomicOr(b.err, kErrLimit);
+          atomicOr(b.err, kErrHuge);
           b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, MG_READ_TOO_LARGE, 0, 0};
         } else {
-          unsigned at = atomicAdd(next_n, 1u);
-          next[at] = r;
+          next[atomicAdd(next_n, 1u)] = r;
         }
       }
     }
     __syncthreads();
     if (!cursor) break;
+  }
+}
+
+// What one read asks of the oversize tier: over both strands the most seeds and the most postings
+// (the bucket sizes of its seeds, each seed hashed as process_strand hashes it: the hash of
+// hash28_dev over the upper-case window, on the reverse strand complemented).
+template <int G>
+__device__ void read_need(const DevIndex& ix, const uint8_t* raw, uint32_t L, RedTmp<G>* red, uint32_t* seeds_out,
+                          uint64_t* post_out) {
+  const uint32_t k = (uint32_t)ix.k, step = (uint32_t)ix.step, hl = (uint32_t)ix.hlen;
+  const uint32_t n_seeds = L > k ? (L - k + step - 1) / step : 0;
+  uint64_t most = 0;
+  for (int strand = 0; strand < 2; strand++) {
+    uint64_t e = 0;
+    for (uint32_t j = threadIdx.x; j < n_seeds; j += G) {
+      const uint32_t p = j * step;  // p + hl <= L: the last seed starts before L - k
+      uint32_t h = 2166136261u;
+      for (uint32_t t = 0; t < hl; t++) {
+        const uint8_t c = strand == 0 ? upper_dev(raw[p + t]) : complement_dev(upper_dev(raw[L - 1 - p - t]));
+        h = (h * 16777619u) ^ c;
+      }
+      h = ((h >> 28) ^ h) & 0x0FFFFFFFu;
+      e += __ldg(ix.dir + h + 1) - __ldg(ix.dir + h);
+    }
+    e = grp_sum_u64<G>(e, red);
+    most = e > most ? e : most;
+  }
+  *seeds_out = n_seeds;
+  *post_out = most;
+}
+
+// Oversize tier over the global tier's leftovers: a block per read (work stealing), each block
+// with its own workspace slab (hws; null before the first oversize read). A read that does not
+// fit records what it needs in need[0..3] (most bases, seeds, postings; reads waiting) and sets
+// kErrHuge, so that the host grows the slabs and runs the batch again; a read beyond the hard
+// limits, or with more than 65,535 candidates on a strand, is refused (kErrLimit).
+template <int G>
+__global__ void __launch_bounds__(G) k_classify_huge(DevIndex ix, BatchDev b, StageDev sd, const uint32_t* list,
+                                                      const unsigned* list_n, unsigned* cursor, uint8_t* hws,
+                                                      WsLayout lay, Caps caps, unsigned* need) {
+  __shared__ uint32_t s_item;
+  __shared__ RedTmp<G> red;
+  uint8_t* base = hws ? hws + (size_t)blockIdx.x * lay.total : nullptr;
+  StrandWS ws{};
+  if (base) ws = ws_from(base, lay, caps.c);
+  const unsigned n = *list_n;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(cursor, 1u);
+    __syncthreads();
+    const unsigned item = s_item;
+    __syncthreads();
+    if (item >= n) break;
+    const uint32_t r = list[item];
+    if (base && process_read<G, true>(ix, b, r, ws, caps, &red, sd.stage, sd.arena, sd.arena_cap, sd.arena_n, b.err))
+      continue;
+    const uint64_t o0 = b.offs[r], Lr = b.offs[r + 1] - o0;
+    uint32_t seeds = 0;
+    uint64_t post = 0;
+    if (Lr <= kHugeMaxQ) read_need<G>(ix, b.bases + o0, (uint32_t)Lr, &red, &seeds, &post);
+    if (threadIdx.x == 0) {
+      const bool hard = Lr > kHugeMaxQ || post > kHugeMaxE;
+      const bool grow = !hard && (Lr > (uint64_t)caps.q || seeds > (uint32_t)caps.seeds || post > (uint64_t)caps.e);
+      if (grow) {
+        atomicMax(need + 0, (unsigned)Lr);
+        atomicMax(need + 1, seeds);
+        atomicMax(need + 2, (unsigned)post);
+        atomicAdd(need + 3, 1u);
+        atomicOr(b.err, kErrHuge);
+      } else {
+        atomicOr(b.err, kErrLimit);
+      }
+      b.reads[r] = mg_read_result{-1.0f, 0, 0, 0, MG_READ_TOO_LARGE, 0, 0};
+    }
+    __syncthreads();
   }
 }
 
@@ -1109,7 +1197,7 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
   }
   if (w.stage.alloc(n_reads * kSlots * sizeof(mg_candidate) + 16) ||
       w.arena.alloc(arena_cap * sizeof(mg_candidate)) || w.ctr.alloc(256) ||
-      w.ovf.alloc(7 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
+      w.ovf.alloc(8 * (n_reads + 4) * 4 + 16) || w.sums.alloc(((n_reads + kScanBlock - 1) / kScanBlock + 1) * 8))
     return set_error(MG_ERR_OOM, "staging buffers");
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   if (w.gws.alloc(l3.total * kB3Blocks)) return set_error(MG_ERR_OOM, "global workspace");
@@ -1119,7 +1207,8 @@ int ensure_workspace(Workspace& w, uint64_t n_reads, uint64_t n_bases, bool host
 // Counters in w_ctr (device): 0 n_cands(u64) | 8 arena_n(u64) | 16 err | 20 work | 24 n_ovf1 |
 // 28 work2 | 32 n_ovf2 | 36 work3 | 40 total(u64) | 48 n_ovf0 | 52 work1 | 56 n_ovf0b | 60 work0b |
 // 64 n_ovf1b | 68 work of the smaller long-read size | 72 n_ovf0c | 76 work0c | 80 n_ovf1c |
-// 84 work of the larger long-read size
+// 84 work of the larger long-read size | 88 n_ovf3 (the global tier's leftovers) | 92 work4 |
+// 96 oversize need: most bases, seeds, postings, reads waiting (4 x u32)
 int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs, const uint8_t* d_bases,
                         mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st,
                         bool plain, unsigned long long* chain, const ChainSync* cs) {
@@ -1156,6 +1245,10 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   uint32_t* ovf1c = w.ovf.as<uint32_t>() + 6 * (n + 4);  // the smaller long-read size's leftovers
   unsigned* n_ovf1c = (unsigned*)(ctr + 80);
   unsigned* work_long2 = (unsigned*)(ctr + 84);
+  uint32_t* ovf3 = w.ovf.as<uint32_t>() + 7 * (n + 4);  // the global tier's leftovers
+  unsigned* n_ovf3 = (unsigned*)(ctr + 88);
+  unsigned* work4 = (unsigned*)(ctr + 92);
+  unsigned* huge_need = (unsigned*)(ctr + 96);
   StageDev sd;
   sd.stage = w.stage.as<mg_candidate>();
   sd.arena = w.arena.as<mg_candidate>();
@@ -1166,6 +1259,8 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
   const WsLayout l2 = ws_layout(kB2Q, kB2Seeds, kB2E, kB2C);
   const WsLayout l3 = ws_layout(kB3Q, kB3Seeds, kB3E, kB3C);
   const Caps c2{kB2Q, kB2Seeds, kB2E, kB2C}, c3{kB3Q, kB3Seeds, kB3E, kB3C};
+  const WsLayout lh = ws_layout((int)w.hq, (int)w.hseeds, (int)w.he, (int)w.hc, true);
+  const Caps ch{(int)w.hq, (int)w.hseeds, (int)w.he, (int)w.hc};
   static bool attr_set = false;
   if (!attr_set) {
     CU(cudaFuncSetAttribute(k_classify_block<kB2Threads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l2.total));
@@ -1181,8 +1276,13 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
     // ev[3..4] block tier, ev[4..5] global tier, ev[6..7] compaction
     if (tm) CU(cudaEventRecord(ix->ev[0], st));
     auto global_tier = [&](cudaStream_t s) {
-      k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, s>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3, nullptr,
-                                                                    nullptr, w.gws.as<uint8_t>(), l3, c3, 1);
+      k_classify_block<kB3Threads><<<kB3Blocks, kB3Threads, 0, s>>>(ix->dix, b, sd, b.ovf2, b.n_ovf2, b.work3, ovf3,
+                                                                    n_ovf3, w.gws.as<uint8_t>(), l3, c3, !w.hmode);
+      // the oversize tier, once a batch of this workspace has needed it: one block while it has
+      // no workspace (it only sizes the reads it gets)
+      if (w.hmode)
+        k_classify_huge<kHugeThreads><<<(unsigned)std::max(1, w.hslabs), kHugeThreads, 0, s>>>(
+            ix->dix, b, sd, ovf3, n_ovf3, work4, w.hslabs ? w.hws.as<uint8_t>() : nullptr, lh, ch, huge_need);
     };
     if (plain) {
       // every read gets its own block (one launch for the batch)
@@ -1253,15 +1353,39 @@ int run_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_offs,
 }
 
 int read_counters(Workspace& w, cudaStream_t st, Counters* c) {
-  uint8_t h[64];
-  CU(cudaMemcpyAsync(h, w.ctr.p, 64, cudaMemcpyDeviceToHost, st));
+  uint8_t h[112];
+  CU(cudaMemcpyAsync(h, w.ctr.p, 112, cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   unsigned long long total, need;
   std::memcpy(&c->err, h + 16, 4);
   std::memcpy(&need, h + 8, 8);
   std::memcpy(&total, h + 40, 8);
+  std::memcpy(c->huge_need, h + 96, 16);
   c->n_cands = total;
   c->arena_need = need;
+  return MG_OK;
+}
+
+// Grow the oversize tier's slabs to hold every read the last run sized (and every read the old
+// slabs held): one slab per waiting read, up to kHugeMaxSlabs and kHugeMaxBytes in all.
+static int grow_oversize(mg_index* ix, Workspace& w, const Counters& c) {
+  const uint32_t q = std::max(w.hq, c.huge_need[0]), seeds = std::max(w.hseeds, c.huge_need[1]);
+  uint32_t e = 1;
+  while (e < std::max(w.he, c.huge_need[2])) e <<= 1;
+  const uint32_t cand = std::min<uint32_t>(std::min<uint32_t>(e, std::max<uint32_t>(ix->dix.n_refs, 1)), 65535);
+  const WsLayout l = ws_layout((int)q, (int)seeds, (int)e, (int)cand, true);
+  const uint64_t fit = std::max<uint64_t>(1, kHugeMaxBytes / l.total);
+  const int slabs = (int)std::min<uint64_t>(std::min<uint64_t>(std::max<uint64_t>(w.hslabs, c.huge_need[3]), kHugeMaxSlabs), fit);
+  if (w.hws.alloc(l.total * (size_t)slabs)) {
+    w.hslabs = 0;
+    w.hq = w.hseeds = w.he = w.hc = 0;
+    return set_error(MG_ERR_OOM, "oversize-read workspace");
+  }
+  w.hslabs = slabs;
+  w.hq = q;
+  w.hseeds = seeds;
+  w.he = e;
+  w.hc = cand;
   return MG_OK;
 }
 
@@ -1269,12 +1393,25 @@ int complete_pipeline(mg_index* ix, Workspace& w, uint64_t n, const uint64_t* d_
                       mg_read_result* d_reads, mg_candidate* d_out, uint64_t cap, cudaStream_t st, bool plain,
                       Counters* c) {
   int rc = read_counters(w, st, c);
-  if (rc || !(c->err & kErrArena)) return rc;
-  if (w.arena.alloc((c->arena_need + (c->arena_need >> 3) + 1024) * sizeof(mg_candidate)))
-    return set_error(MG_ERR_OOM, "staging arena");
-  rc = run_pipeline(ix, w, n, d_offs, d_bases, d_reads, d_out, cap, st, plain);
-  c->reran = true;
-  return rc ? rc : read_counters(w, st, c);
+  // a rerun can need another: the first oversize read turns the oversize tier on, its next run
+  // sizes the reads, and their candidates go to the arena only once they fit
+  for (int attempt = 0; rc == MG_OK && attempt < 4 && (c->err & (kErrArena | kErrHuge)); attempt++) {
+    if ((c->err & kErrArena) &&
+        w.arena.alloc((c->arena_need + (c->arena_need >> 3) + 1024) * sizeof(mg_candidate)))
+      return set_error(MG_ERR_OOM, "staging arena");
+    if (c->err & kErrHuge) {
+      if (!w.hmode) {
+        w.hmode = 1;
+      } else {
+        rc = grow_oversize(ix, w, *c);
+        if (rc) return rc;
+      }
+    }
+    rc = run_pipeline(ix, w, n, d_offs, d_bases, d_reads, d_out, cap, st, plain);
+    c->reran = true;
+    if (rc == MG_OK) rc = read_counters(w, st, c);
+  }
+  return rc;
 }
 
 int finish_errors(Workspace& w, cudaStream_t st, uint64_t* n_cands) {
@@ -1290,6 +1427,7 @@ int error_status(int err) {
   if (err & kErrOutput) return set_error(MG_ERR_OOM, "candidate output buffer too small");
   if (err & kErrLogRange) return set_error(MG_ERR_LIMIT, "relative-score logarithm outside its exact domain");
   if (err & kErrArena) return set_error(MG_ERR_OOM, "staging arena too small");
+  if (err & kErrHuge) return set_error(MG_ERR_LIMIT, "a read needs a larger oversize-read workspace");
   if (err & kErrInternal) return set_error(MG_ERR_CUDA, "a device loop reached its bound (internal error)");
   return MG_OK;
 }
@@ -1491,7 +1629,7 @@ static int classify_chunked(mg_index* ix, Workspace& w, const mg_batch* batch, m
   int err = 0;
   std::memcpy(&err, &h[1], 4);
   out->n_cands = h[0];
-  if (err & kErrArena) return kRunWhole;
+  if (err & (kErrArena | kErrHuge)) return kRunWhole;
   return error_status(err);
 }
 
@@ -1535,6 +1673,22 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   // arena the whole batch needed (no chunk needs more), so that batches like this one stay in
   // chunks from now on (a failed allocation only leaves them on this path)
   if (chunks_overflowed && ix->ws2.arena.alloc(w.arena.n)) cudaGetLastError();  // not sticky: clear it
+  // the same for the oversize tier's slabs (the even chunks run on w itself)
+  if (chunks_overflowed && w.hmode) ix->ws2.hmode = 1;
+  if (chunks_overflowed && w.hslabs > 0 && ix->ws2.hws.n < w.hws.n) {
+    Workspace& o = ix->ws2;
+    if (o.hws.alloc(w.hws.n)) {
+      cudaGetLastError();
+      o.hslabs = 0;
+      o.hq = o.hseeds = o.he = o.hc = 0;
+    } else {
+      o.hslabs = w.hslabs;
+      o.hq = w.hq;
+      o.hseeds = w.hseeds;
+      o.he = w.he;
+      o.hc = w.hc;
+    }
+  }
   if (n) {
     CU(cudaMemcpyAsync(out->reads, w.reads.p, n * sizeof(mg_read_result), cudaMemcpyDeviceToHost, st));
     if (total) CU(cudaMemcpyAsync(out->cands, w.cands.p, total * sizeof(mg_candidate), cudaMemcpyDeviceToHost, st));

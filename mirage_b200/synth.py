@@ -384,6 +384,26 @@ def workload(name: str, scale: float = 1.0, seed: int = 1, n_reads: int | None =
                                       lambda n: _lognormal_lengths(rng, n, 5000, 0.8, lo=1000, hi=20000),
                                       rng, sub=0.03, indel=0.02, chimera_frac=0.1)
         return refs, reads, truth
+    if name == "ultralong":
+        # reads past 65,535 bases (the oversize tier): references of 270 kb and more, reads of
+        # 66-250 kb with 3% substitutions, 2% indels and chimeras, one unrelated read, and a few
+        # short reads beside them in the batch
+        n_refs = max(4, int(round(16 * scale)))
+        lens = _lognormal_lengths(rng, n_refs, 400_000, 0.3, lo=270_000)
+        refs = make_references(n_refs, lens, rng.uniform(0.35, 0.65, size=n_refs), rng)
+        nr = n_reads if n_reads is not None else int(round(12 * scale))
+        n_short = nr // 4
+        n_unrel = 1 if nr >= 4 else 0
+        long_reads, truth = make_reads(refs, nr - n_short - n_unrel, n_unrel,
+                                       lambda n: rng.integers(66_000, 250_001, size=n), rng,
+                                       sub=0.03, indel=0.02, chimera_frac=0.25)
+        short_reads, t2 = make_reads(refs, n_short, 0, lambda n: rng.integers(150, 20_001, size=n), rng,
+                                     sub=0.01, indel=0.005)
+        seqs = [long_reads.seq(i) for i in range(len(long_reads))] + [short_reads.seq(i) for i in range(len(short_reads))]
+        offs = np.zeros(len(seqs) + 1, dtype=np.uint64)
+        offs[1:] = np.cumsum([len(x) for x in seqs])
+        reads = SeqSet(np.concatenate(seqs), offs, [b"read%d" % i for i in range(len(seqs))])
+        return refs, reads, np.concatenate([truth, t2])
     if name == "repeats":
         n_refs = max(4, int(round(20_000 * scale)))
         lens = _lognormal_lengths(rng, n_refs, 80_000, 0.67, lo=6000)

@@ -39,6 +39,8 @@ CASES = {
     "long_small": ("long", 0.004, 3, 150, 4),
     "repeats_small": ("repeats", 0.002, 4, 2000, 4),
     "plain64": ("plain", 0.25, 5, 1500, 8),
+    # reads past 65,535 bases (66-250 kb, chimeras, one unrelated) beside short ones
+    "ultralong_small": ("ultralong", 1.0, 7, 12, 4),
     # the benchmark's own reference set at full scale (5,000 references, 344 Mbp: about 1.3
     # postings per 28-bit hash, the dense-bucket regime no smaller case reaches) with 20,000 reads
     "uneven_full": ("uneven_fast", 1.0, 2024, 20000, 8),

@@ -486,3 +486,77 @@ def test_long_reads_chunked_by_bases(golden):
         ix.set_tuning()
     assert np.array_equal(chunked.reads.view(np.uint8), whole.reads.view(np.uint8))
     assert np.array_equal(chunked.cands.view(np.uint8), whole.cands.view(np.uint8))
+
+
+@pytest.mark.parametrize("form", ["batched", "plain"])
+def test_reads_past_65535_bases(tmp_path, form):
+    """Reads of 65,535 bases (the global tier's last length) to 300 kb on four identical 400 kb
+    references and a fifth, different one: from 65,536 bases on they go to the oversize tier,
+    which the first call turns on, sizes and grows, running the batch again each time. Every
+    result equals the oracle's, with substitutions and lowercase bases in some reads, every read
+    is assigned, and a second call on the grown workspace repeats the first byte for byte."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(61)
+    acgt = np.frombuffer(b"ACGT", np.uint8)
+    core = acgt[rng.integers(0, 4, 400_000)]
+    refs = [core] * 4 + [acgt[rng.integers(0, 4, 400_000)]]
+    offs = np.zeros(len(refs) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(r) for r in refs])
+    image = M.build_image(np.concatenate(refs), offs, [f"ref{i}" for i in range(len(refs))])
+    path = tmp_path / "four.mhm"
+    image.tofile(path)
+    gix = M.Index(image)
+    oix = O.Index(str(path))
+    seqs = []
+    for n in (65_535, 65_536, 70_000, 131_072, 300_000):
+        s0 = int(rng.integers(0, 400_000 - n))
+        r = core[s0:s0 + n].copy()
+        hit = rng.random(n) < 0.02
+        r[hit] = acgt[(np.searchsorted(acgt, r[hit]) + 1) % 4]
+        seqs.append(r.tobytes())
+    seqs.append(seqs[2].lower())
+    seqs.append(refs[4][5000:105000].tobytes())
+    seqs.append(core[1000:1150].tobytes())
+    first = check_against_oracle(gix, oix, seqs, form=form)
+    assert first.reads["reported"].all()
+    data, roffs = csr(seqs)
+    _same(first, gix.classify(data, roffs, form=form))
+
+
+def test_reads_past_65535_bases_in_chunks(golden):
+    """A host-buffer batch of 66-250 kb reads large enough for chunks: a chunk meets reads that the
+    oversize tier has no workspace for yet, so the call runs the batch in one piece, which grows
+    it (and the odd chunks' workspace); the next call stays in chunks. Both equal the batch in one
+    piece, byte for byte, and repeat the reference's results for the first copy."""
+    g = golden("ultralong_small")
+    ix = M.Index(g.image)
+    reps = max(1, int(np.ceil(30e6 / float(g.reads.offs[-1]))))
+    data, offs = _tile(g.reads.data, g.reads.offs, reps)
+    assert offs[-1] > 2 * 65536 * 192
+    first = ix.classify(data, offs)
+    second = ix.classify(data, offs)
+    ix.set_tuning(chunks=1)
+    try:
+        whole = ix.classify(data, offs)
+    finally:
+        ix.set_tuning()
+    _same(first, whole)
+    _same(second, whole)
+    one = ix.classify(g.reads.data, g.reads.offs)
+    d = diff(canon_from_gpu(one), canon_from_dump(g.dump))
+    assert not d, "\n".join(d)
+
+
+def test_read_beyond_the_oversize_limit_is_refused(golden):
+    """A read of 2,000,001 bases (past the oversize tier's 2,000,000) fails the call with
+    MG_ERR_LIMIT and is marked MG_READ_TOO_LARGE; a read of 200 kb in the same index works."""
+    g, (gix, _) = plain_index(golden)
+    rng = np.random.default_rng(5)
+    big = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 2_000_001)].tobytes()
+    data, offs = csr([big])
+    with pytest.raises(M.MirageError) as e:
+        gix.classify(data, offs)
+    assert e.value.code == -4
+    data, offs = csr([big[:200_000]])
+    gix.classify(data, offs)
