@@ -236,7 +236,8 @@ int mg_classify_device(mg_index* ix, uint64_t n_reads, const uint64_t* d_offsets
 /* Waits for work queued by mg_classify_device on `stream` and reports its errors; *n_cands
  * receives the number of candidates written. It completes the index's last mg_classify_device
  * launch, whose device buffers must stay valid until it returns: a batch whose reads have more
- * candidates than the internal staging area held is run again here with a larger one. */
+ * candidates than the internal staging area held, or that holds reads for the oversize tier
+ * beyond its current workspace (see mg_score_batch), is run again here once that has grown. */
 int mg_classify_device_sync(mg_index* ix, void* stream, uint64_t* n_cands);
 
 /* Scoring-only drop-in for MatrixCPU::CPUGetHighestScore (MatrixCPU.cpp:417) when the

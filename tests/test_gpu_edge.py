@@ -550,7 +550,7 @@ def test_reads_past_65535_bases_in_chunks(golden):
 
 def test_read_beyond_the_oversize_limit_is_refused(golden):
     """A read of 2,000,001 bases (past the oversize tier's 2,000,000) fails the call with
-    MG_ERR_LIMIT and is marked MG_READ_TOO_LARGE; a read of 200 kb in the same index works."""
+    MG_ERR_LIMIT; a read of 200 kb on the same index then classifies."""
     g, (gix, _) = plain_index(golden)
     rng = np.random.default_rng(5)
     big = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 2_000_001)].tobytes()
