@@ -22,7 +22,11 @@ struct DevBuf {
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
-    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return -1;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) {
+      cudaGetLastError();  // an allocation failure is not sticky: clear it for the next launch check
+      p = nullptr;
+      return -1;
+    }
     n = bytes;
     return 0;
   }

@@ -1672,13 +1672,12 @@ static int classify_host(mg_index* ix, const mg_batch* batch, mg_result* out, bo
   // a chunk's staging arena ran out: the odd chunks' workspace, sized for one chunk, gets the
   // arena the whole batch needed (no chunk needs more), so that batches like this one stay in
   // chunks from now on (a failed allocation only leaves them on this path)
-  if (chunks_overflowed && ix->ws2.arena.alloc(w.arena.n)) cudaGetLastError();  // not sticky: clear it
+  if (chunks_overflowed) ix->ws2.arena.alloc(w.arena.n);
   // the same for the oversize tier's slabs (the even chunks run on w itself)
   if (chunks_overflowed && w.hmode) ix->ws2.hmode = 1;
   if (chunks_overflowed && w.hslabs > 0 && ix->ws2.hws.n < w.hws.n) {
     Workspace& o = ix->ws2;
     if (o.hws.alloc(w.hws.n)) {
-      cudaGetLastError();
       o.hslabs = 0;
       o.hq = o.hseeds = o.he = o.hc = 0;
     } else {
